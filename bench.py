@@ -1,0 +1,312 @@
+#!/usr/bin/env python
+"""Benchmark: microseconds per Lucas-Lehmer iteration at the 8M-point NTT.
+
+Workload: the Lucas-Lehmer test of q = 139000003 (the first prime above 1.39e8)
+at the reference's length n = 2^23 (ntt_lengths.cu:88-98 picks it), from
+s0 = 4.  One step = ITERATIONS_PER_STEP squarings (-2 each) of that residue.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value`: device time of the K steps (CUDA events on the test's stream, residue
+resident in HBM, L2 flushed between steps) per squaring.  `e2e`: the same
+through the C ABI with host buffers -- every step uploads the residue from
+pinned memory (lnt_set_digits), squares, and reads the canonical residue back
+(lnt_get_digits).  With N > 1 every rank runs an independent replica (one LL
+test does not shard); the time is the max over ranks.
+
+--impl reference times the reference's algorithm on the host cores: the
+reference has no CPU implementation, so this is the CPU oracle
+(oracle/lnt_oracle.c, a port of its per-iteration arithmetic) on all threads.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+EXPONENT = 139000003
+LOG2N = 23
+N = 1 << LOG2N
+ITERATIONS_PER_STEP = 1000
+METRIC = "µs/iteration at 8M-pt NTT"
+UNIT = "us/iteration"
+FLUSH_BYTES = 256 << 20  # larger than the 126 MB L2
+ALGO_BYTES_PER_WORD_PER_SWEEP = 16  # one read + one write of a uint64 word
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--iterations-per-step", type=int, default=ITERATIONS_PER_STEP)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def rank_info():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)),
+            int(os.environ.get("WORLD_SIZE", 1)))
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.device)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, or None."""
+    p = ROOT / "profiles" / "ncu_traffic.json"
+    if not p.exists():
+        return None
+    d = json.loads(p.read_text())
+    v = d.get("kernels", {}).get(kernel)
+    return None if v is None else float(v)
+
+
+def cpu_port_sample(threads: int, iterations: int):
+    """Time the CPU oracle on `iterations` LL squarings of the workload."""
+    from oracle import oracle as O
+
+    O.set_threads(threads)
+    with O.OracleTest(EXPONENT, N, prp=False) as T:
+        T.iterate(1)  # warm caches and the thread pool
+        t0 = time.perf_counter()
+        T.iterate(iterations)
+        dt = time.perf_counter() - t0
+    return dt * 1e6 / iterations
+
+
+def run_reference(args, rank, world):
+    """CPU reference arm: the oracle port on all host threads."""
+    if rank != 0:
+        return
+    from oracle import oracle as O
+
+    threads = O.max_threads()
+    per_step = 3
+    O.set_threads(threads)
+    with O.OracleTest(EXPONENT, N, prp=False) as T:
+        for _ in range(args.warmup):
+            T.iterate(per_step)
+        times = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            T.iterate(per_step)
+            times.append(time.perf_counter() - t0)
+    us = sum(times) * 1e6 / (args.steps * per_step)
+    sample = f"{per_step} LL squarings of q={EXPONENT} at n=2^{LOG2N} per step"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": us, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sum(times) * 1e3 / args.steps,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic: LL residue sequence from s0 = 4",
+        "config": {"workload": f"LL q={EXPONENT} n=2^{LOG2N} (8M-pt NTT)", "exponent": EXPONENT,
+                   "n": N, "iterations_per_step": per_step,
+                   "implementation": "CPU oracle port of the reference arithmetic (reference has no CPU path)"},
+        "cpu_baseline": {"value": us, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": us, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    rank, local_rank, world = rank_info()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+
+    import cuda_b200
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    ips = args.iterations_per_step
+
+    stream = torch.cuda.Stream(device=dev)
+    test = cuda_b200.LucasTest(EXPONENT, N, prp=False, device=local_rank)
+    test.set_stream(stream.cuda_stream)
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=dev)
+
+    def flush_l2():
+        with torch.cuda.stream(stream):
+            flush.random_(0, 255)
+
+    # warm-up steps (untimed)
+    for _ in range(args.warmup):
+        flush_l2()
+        test.iterate(ips)
+    stream.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    # ---- device-resident timed region -------------------------------------
+    barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    step_ms, kernels = [], {}
+    for _ in range(args.steps):
+        flush_l2()
+        prof = test.profile_iterations(ips)  # CUDA events between the launches
+        step_ms.append(sum(ms for _, ms in prof.values()))
+        for name, (launches, ms) in prof.items():
+            a = kernels.setdefault(name, [0, 0.0])
+            a[0] += launches
+            a[1] += ms
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    barrier()
+    total_ms = sum(step_ms)
+    if dist is not None:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = total_ms * 1e3 / (world * args.steps * ips)
+
+    # ---- end to end through the C ABI with host buffers --------------------
+    host = torch.empty(N, dtype=torch.int64, pin_memory=True)
+    test.digits(host.numpy().view("uint64"))
+    stream.synchronize()
+    barrier()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    wall0 = time.perf_counter()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        test.set_digits(host.numpy().view("uint64"))
+        test.iterate(ips)
+        test.digits(host.numpy().view("uint64"))
+    ev1.record(stream)
+    ev1.synchronize()
+    wall = time.perf_counter() - wall0
+    e2e_ms = ev0.elapsed_time(ev1)
+    barrier()
+    if dist is not None:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = e2e_ms * 1e3 / (world * args.steps * ips)
+    res64 = test.res64()
+
+    # ---- roofline of the dominant kernel -----------------------------------
+    dom = max(kernels.items(), key=lambda kv: kv[1][1])
+    dom_name, (dom_launches, dom_ms) = dom
+    avg_s = dom_ms / dom_launches / 1e3
+    if test.plan.startswith("TWOPASS"):
+        algo_bytes = ALGO_BYTES_PER_WORD_PER_SWEEP * N  # each pass reads and writes the residue once
+    else:
+        algo_bytes = ALGO_BYTES_PER_WORD_PER_SWEEP * N * ips
+    achieved = algo_bytes / avg_s / 1e9
+    peak, peak_kind = measured_peak_hbm()
+    traffic = ncu_traffic(dom_name)
+    launches_in_timed = sum(a[0] for a in kernels.values())
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sample_iters = 4
+        cpu_us = cpu_port_sample(1, sample_iters)
+        cpu = {"value": cpu_us, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"{sample_iters} LL squarings of q={EXPONENT} at n=2^{LOG2N}, one thread"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic: LL residue sequence from s0 = 4",
+            "config": {"workload": f"LL q={EXPONENT} n=2^{LOG2N} (8M-pt NTT), {ips} squarings per step",
+                       "exponent": EXPONENT, "n": N, "iterations_per_step": ips, "plan": test.plan,
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "flushed between steps (256 MiB write)", "res64_after_run": f"{res64:016x}"},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": N * 8, "d2h_bytes_per_step": N * 8,
+                    "wall_s": wall},
+            "gpu_launches": launches_in_timed,
+            "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "algo_bytes_per_launch": algo_bytes,
+                         "avg_launch_us": avg_s * 1e6},
+            "kernels": {k: {"launches": v[0], "avg_us": v[1] * 1e3 / v[0]} for k, v in kernels.items()},
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    test.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

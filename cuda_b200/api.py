@@ -1,0 +1,206 @@
+"""ctypes binding of liblucasntt.so (C ABI in include/lucasntt.h).
+
+Python face of the reference's LucasPRP / NttLengths interface
+(lucas_prp.cu, ntt_lengths.cu): create a test for an exponent, iterate,
+read the residue back in the reference's dump order.  There is no CPU
+fallback: if the shared library is missing the import fails loudly.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = _HERE / "liblucasntt.so"
+HEADER = _HERE.parent / "include" / "lucasntt.h"
+
+LNT_OK = 0
+LNT_ERR_INVALID_ARGUMENT = 1
+LNT_ERR_UNSUPPORTED_LENGTH = 2
+LNT_ERR_CUDA = 3
+LNT_ERR_OUT_OF_MEMORY = 4
+LNT_ERR_NUMERIC = 5
+LNT_ERR_NO_DEVICE = 6
+LNT_ERR_BUDGET = 7
+
+_lib = None
+
+
+class KernelTime(ctypes.Structure):
+    """lnt_kernel_time: per-kernel-kind CUDA-event totals."""
+    _fields_ = [("name", ctypes.c_char * 32), ("launches", ctypes.c_uint32),
+                ("total_ms", ctypes.c_float)]
+
+
+class LucasNTTError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        L = lib()
+        msg = L.lnt_status_string(status).decode()
+        detail = L.lnt_last_error().decode()
+        super().__init__(f"{where}: {msg}" + (f" ({detail})" if detail else ""))
+        self.status = status
+
+
+def lib() -> ctypes.CDLL:
+    """Load liblucasntt.so; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(f"{LIB_PATH} is missing: build it with `make -C cuda_b200`")
+    L = ctypes.CDLL(str(LIB_PATH))
+    u32, u64, i32, vp, sz = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t
+    cp = ctypes.c_char_p
+    sigs = {
+        "lnt_status_string": ([i32], cp),
+        "lnt_last_error": ([], cp),
+        "lnt_secured_log2_length": ([u32], u32),
+        "lnt_length_candidates": ([u32, cp, sz], i32),
+        "lnt_parse_length": ([cp, ctypes.POINTER(u32)], i32),
+        "lnt_check_provided_length": ([u32, cp, ctypes.POINTER(i32)], i32),
+        "lnt_create": ([u32, u32, i32, i32, ctypes.POINTER(vp)], i32),
+        "lnt_destroy": ([vp], i32),
+        "lnt_init_test": ([vp], i32),
+        "lnt_iterate": ([vp, u64], i32),
+        "lnt_set_digits": ([vp, vp, sz], i32),
+        "lnt_get_digits": ([vp, vp, sz], i32),
+        "lnt_res64": ([vp, ctypes.POINTER(u64)], i32),
+        "lnt_is_prime": ([vp, ctypes.POINTER(i32)], i32),
+        "lnt_get_length": ([vp, ctypes.POINTER(u32)], i32),
+        "lnt_get_raw_state": ([vp, vp, sz], i32),
+        "lnt_get_widths": ([vp, vp, sz], i32),
+        "lnt_plan_name": ([vp, cp, sz], i32),
+        "lnt_set_stream": ([vp, vp], i32),
+        "lnt_synchronize": ([vp], i32),
+        "lnt_profile_iterations": ([vp, u64, ctypes.POINTER(KernelTime), i32, ctypes.POINTER(i32)], i32),
+    }
+    for name, (args, res) in sigs.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def _check(status: int, where: str) -> None:
+    if status != LNT_OK:
+        raise LucasNTTError(status, where)
+
+
+def secured_log2_length(exponent: int) -> int:
+    """NttLengths::GetNttSecuredLength (ntt_lengths.cu:88-98)."""
+    return int(lib().lnt_secured_log2_length(exponent))
+
+
+def length_candidates(exponent: int) -> list[str]:
+    """NttLengths::GetCandidates (ntt_lengths.cu:100-128)."""
+    buf = ctypes.create_string_buffer(1024)
+    lib().lnt_length_candidates(exponent, buf, 1024)
+    return [s for s in buf.value.decode().split(";") if s]
+
+
+def parse_length(description: str) -> int:
+    """NttLengths::StringToLengths + GetTotalLength (ntt_lengths.cu:32-75, :130-142)."""
+    n = ctypes.c_uint32()
+    _check(lib().lnt_parse_length(description.encode(), ctypes.byref(n)), "parse_length")
+    return int(n.value)
+
+
+def check_provided_length(exponent: int, description: str) -> int:
+    """NttLengths::CheckProvidedLength (ntt_lengths.cu:77-86)."""
+    d = ctypes.c_int()
+    _check(lib().lnt_check_provided_length(exponent, description.encode(), ctypes.byref(d)),
+           "check_provided_length")
+    return int(d.value)
+
+
+class LucasTest:
+    """One Lucas-Lehmer (prp=False) or base-3 PRP test of M = 2^exponent - 1."""
+
+    def __init__(self, exponent: int, n: int = 0, prp: bool = False, device: int = 0):
+        h = ctypes.c_void_p()
+        _check(lib().lnt_create(exponent, n, int(bool(prp)), device, ctypes.byref(h)), "lnt_create")
+        self._h = h
+        self.exponent = int(exponent)
+        self.prp = bool(prp)
+        nn = ctypes.c_uint32()
+        _check(lib().lnt_get_length(self._h, ctypes.byref(nn)), "lnt_get_length")
+        self.n = int(nn.value)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().lnt_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def init_test(self) -> None:
+        _check(lib().lnt_init_test(self._h), "lnt_init_test")
+
+    def iterate(self, iterations: int) -> None:
+        _check(lib().lnt_iterate(self._h, int(iterations)), "lnt_iterate")
+
+    def set_digits(self, digits) -> None:
+        d = np.ascontiguousarray(digits, dtype=np.uint64)
+        _check(lib().lnt_set_digits(self._h, d.ctypes.data, d.size), "lnt_set_digits")
+
+    def digits(self, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty(self.n, np.uint64)
+        _check(lib().lnt_get_digits(self._h, out.ctypes.data, out.size), "lnt_get_digits")
+        return out
+
+    def res64(self) -> int:
+        r = ctypes.c_uint64()
+        _check(lib().lnt_res64(self._h, ctypes.byref(r)), "lnt_res64")
+        return int(r.value)
+
+    def is_prime(self) -> bool:
+        r = ctypes.c_int()
+        _check(lib().lnt_is_prime(self._h, ctypes.byref(r)), "lnt_is_prime")
+        return bool(r.value)
+
+    def raw_state(self) -> np.ndarray:
+        """Internal signed words (diagnostic; see lnt_get_raw_state)."""
+        out = np.empty(self.n, np.int64)
+        _check(lib().lnt_get_raw_state(self._h, out.ctypes.data, out.size), "lnt_get_raw_state")
+        return out
+
+    def widths(self) -> np.ndarray:
+        w = np.empty(self.n, np.uint8)
+        _check(lib().lnt_get_widths(self._h, w.ctypes.data, w.size), "lnt_get_widths")
+        return w
+
+    @property
+    def plan(self) -> str:
+        buf = ctypes.create_string_buffer(64)
+        _check(lib().lnt_plan_name(self._h, buf, 64), "lnt_plan_name")
+        return buf.value.decode()
+
+    def set_stream(self, stream_handle: int | None) -> None:
+        _check(lib().lnt_set_stream(self._h, stream_handle), "lnt_set_stream")
+
+    def synchronize(self) -> None:
+        _check(lib().lnt_synchronize(self._h), "lnt_synchronize")
+
+    def profile_iterations(self, iterations: int) -> dict[str, tuple[int, float]]:
+        """Squarings with CUDA events between launches: {kernel: (launches, total_ms)}."""
+        cap = 16
+        arr = (KernelTime * cap)()
+        count = ctypes.c_int()
+        _check(lib().lnt_profile_iterations(self._h, int(iterations), arr, cap, ctypes.byref(count)),
+               "lnt_profile_iterations")
+        return {arr[i].name.decode(): (int(arr[i].launches), float(arr[i].total_ms))
+                for i in range(min(cap, count.value))}

@@ -1,0 +1,97 @@
+// Exact arithmetic modulo the Goldilocks prime p = 2^64 - 2^32 + 1.
+//
+// Replaces the reference's common/arithmetics.cuh:26-312 (add_Mod, sub_Mod,
+// mul_Mod, pow_Mod, inv_Mod and the shift24/48/72 family).  Written from the
+// two identities 2^64 == 2^32 - 1 and 2^96 == -1 (mod p); every function keeps
+// its result canonical in [0, p).  The functions are __host__ __device__ so the
+// CPU test suite checks them bit-for-bit against the oracle.
+#pragma once
+#include <stdint.h>
+
+#if defined(__CUDACC__)
+#define GL_HD __host__ __device__ __forceinline__
+#else
+#define GL_HD static inline
+#endif
+
+namespace gl {
+
+constexpr uint64_t P = 0xFFFFFFFF00000001ull;
+constexpr uint64_t EPS = 0x00000000FFFFFFFFull;  // 2^64 mod p
+constexpr uint64_t HALF = P >> 1;                // values above this are negative
+
+GL_HD uint64_t mulhi(uint64_t a, uint64_t b) {
+#if defined(__CUDA_ARCH__)
+  return __umul64hi(a, b);
+#else
+  return (uint64_t)(((unsigned __int128)a * b) >> 64);
+#endif
+}
+
+GL_HD uint64_t add(uint64_t a, uint64_t b) {
+  uint64_t s = a + b;
+  // s < a: the sum wrapped past 2^64, and s - p == s + EPS is the answer.
+  return (s < a || s >= P) ? s - P : s;
+}
+
+GL_HD uint64_t sub(uint64_t a, uint64_t b) {
+  uint64_t d = a - b;
+  return (a < b) ? d + P : d;
+}
+
+GL_HD uint64_t neg(uint64_t a) { return a ? P - a : 0; }
+
+// lo + 2^64 * hi, with hi = h1 * 2^32 + h0, is lo + h0 * (2^32 - 1) - h1.
+GL_HD uint64_t reduce128(uint64_t lo, uint64_t hi) {
+  uint64_t h1 = hi >> 32, h0 = hi & 0xFFFFFFFFull;
+  uint64_t t = lo - h1;
+  if (lo < h1) t -= EPS;  // borrow: t - 2^64 == t - EPS (mod p)
+  uint64_t m = (h0 << 32) - h0;
+  uint64_t r = t + m;
+  if (r < m) r += EPS;    // carry: r + 2^64 == r + EPS (mod p)
+  return r >= P ? r - P : r;
+}
+
+GL_HD uint64_t mul(uint64_t a, uint64_t b) { return reduce128(a * b, mulhi(a, b)); }
+
+GL_HD uint64_t sqr(uint64_t a) { return mul(a, a); }
+
+GL_HD uint64_t pow(uint64_t a, uint64_t e) {
+  uint64_t r = 1;
+  while (e) {
+    if (e & 1) r = mul(r, a);
+    a = mul(a, a);
+    e >>= 1;
+  }
+  return r;
+}
+
+GL_HD uint64_t inv(uint64_t a) { return pow(a, P - 2); }
+
+// x * 2^s for 0 <= s < 192 (2 has multiplicative order 192 modulo p).
+// Only shifts and adds: no multiplier.
+GL_HD uint64_t mul_pow2(uint64_t x, unsigned s) {
+  bool negate = false;
+  if (s >= 96) { s -= 96; negate = true; }  // 2^96 == -1
+  uint64_t r;
+  if (s == 0) {
+    r = x;
+  } else if (s < 64) {
+    r = reduce128(x << s, x >> (64 - s));
+  } else {
+    // x 2^s = (hi 2^64 + lo) 2^64 with (hi, lo) = x 2^k, k = s - 64 < 32;
+    // 2^128 == -2^32, so this is reduce(lo 2^64) - hi 2^32 with hi 2^32 < p.
+    unsigned k = s - 64;
+    uint64_t lo = x << k, hi = k ? (x >> (64 - k)) : 0;
+    r = sub(reduce128(0, lo), hi << 32);
+  }
+  return negate ? neg(r) : r;
+}
+
+// Balanced digit d (|d| < 2^62) as a field element.
+GL_HD uint64_t from_signed(int64_t d) { return d >= 0 ? (uint64_t)d : (uint64_t)d + P; }
+
+// Field element as a signed integer in (-p/2, p/2].
+GL_HD int64_t to_signed(uint64_t c) { return c > HALF ? (int64_t)(c - P) : (int64_t)c; }
+
+}  // namespace gl

@@ -1,0 +1,584 @@
+// C ABI of the single-test path: context lifetime, residue I/O, iteration.
+//
+// Mirrors LucasPRP (lucas_prp.cu:24-346): Initialize allocates the residue and
+// the IBDWT tables, InitializeTest writes the start value, MainLoop queues
+// `iterations` squarings, and readout copies the canonical digits back.
+// Errors are status codes (the reference throws std::runtime_error from
+// cudaCheckErrors, common/common.cuh:23-29).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/lucasntt.h"
+#include "goldilocks.cuh"
+#include "lnt_internal.h"
+
+struct lnt_test {
+  uint32_t q = 0, n = 0;
+  int prp = 0;
+  int device = 0;
+  lnt::Plan plan;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+
+  int64_t* x = nullptr;
+  uint64_t* w = nullptr;
+  uint64_t* uw = nullptr;
+  uint8_t* widths = nullptr;
+  uint32_t* status = nullptr;
+  // resident plan
+  uint64_t* rt = nullptr;
+  uint64_t* irt = nullptr;
+  lnt::ResidentDesc* rdesc = nullptr;
+  // two-pass plan
+  uint64_t *twf = nullptr, *twi = nullptr;
+  uint64_t *rt1 = nullptr, *irt1 = nullptr, *rt2 = nullptr, *irt2 = nullptr;
+  int64_t* carry = nullptr;
+  // canonical readout
+  uint64_t* canon = nullptr;
+  int64_t* blk_carry = nullptr;
+  uint8_t* blk_fn = nullptr;
+  int8_t* blk_cin = nullptr;
+  uint32_t* cflags = nullptr;
+  uint32_t* h_pinned = nullptr;  // 2 words: status, canon flags
+
+  std::vector<uint8_t> h_widths;
+  bool canonical_input = true;  // digits non-negative: next squaring reads outputs unsigned
+  bool pending_carries = false; // two-pass: carry buffer holds carries not yet applied
+  bool pristine = true;         // no squaring since the digits were set
+  bool zero_start = false;      // digits were set to all zero
+  bool canon_valid = false;     // `canon` holds the canonical digits of the current state
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int status, const std::string& msg) {
+  g_last_error = msg;
+  return status;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  return fail(e == cudaErrorMemoryAllocation ? LNT_ERR_OUT_OF_MEMORY : LNT_ERR_CUDA,
+              std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define LNT_CUDA(call, what)                          \
+  do {                                                \
+    cudaError_t e_ = (call);                          \
+    if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+  } while (0)
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+template <class T>
+cudaError_t dalloc(T** p, size_t count) {
+  return cudaMalloc((void**)p, count * sizeof(T));
+}
+
+void free_all(lnt_test* t) {
+  void* ptrs[] = {t->x, t->w, t->uw, t->widths, t->status, t->rt, t->irt, t->rdesc,
+                  t->twf, t->twi, t->rt1, t->irt1, t->rt2, t->irt2, t->carry, t->canon,
+                  t->blk_carry, t->blk_fn, t->blk_cin, t->cflags};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (t->h_pinned) cudaFreeHost(t->h_pinned);
+  if (t->own_stream && t->stream) cudaStreamDestroy(t->stream);
+}
+
+// omega_n^k for k < max(n/2, 1), generator 554 (pre_calculation.cu:61-66).
+void root_table(uint32_t n, bool inverse, std::vector<uint64_t>& out) {
+  uint64_t r = gl::pow(554, (gl::P - 1) / n);
+  if (inverse) r = gl::inv(r);
+  size_t half = n > 1 ? n / 2 : 1;
+  out.resize(half);
+  out[0] = 1;
+  for (size_t k = 1; k < half; ++k) out[k] = gl::mul(out[k - 1], r);
+}
+
+int upload_roots(lnt_test* t, uint32_t n, uint64_t** rt, uint64_t** irt) {
+  std::vector<uint64_t> a, b;
+  root_table(n, false, a);
+  root_table(n, true, b);
+  LNT_CUDA(dalloc(rt, a.size()), "cudaMalloc roots");
+  LNT_CUDA(dalloc(irt, b.size()), "cudaMalloc roots");
+  LNT_CUDA(cudaMemcpy(*rt, a.data(), a.size() * 8, cudaMemcpyHostToDevice), "copy roots");
+  LNT_CUDA(cudaMemcpy(*irt, b.data(), b.size() * 8, cudaMemcpyHostToDevice), "copy roots");
+  return LNT_OK;
+}
+
+lnt::TwoPassDesc twopass_desc(const lnt_test* t) {
+  lnt::TwoPassDesc d{};
+  d.x = t->x;
+  d.carry = t->carry;
+  d.w = t->w;
+  d.uw = t->uw;
+  d.widths = t->widths;
+  d.twf = t->twf;
+  d.twi = t->twi;
+  d.rt1 = t->rt1;
+  d.irt1 = t->irt1;
+  d.rt2 = t->rt2;
+  d.irt2 = t->irt2;
+  d.status = t->status;
+  d.n1 = t->plan.n1;
+  d.n2 = t->plan.n2;
+  d.log2n1 = t->plan.log2n1;
+  d.log2n2 = t->plan.log2n2;
+  d.tile = t->plan.tile;
+  d.ntiles = t->plan.ntiles;
+  d.prp = (uint32_t)t->prp;
+  return d;
+}
+
+// Exact cyclic normalisation on the host: the fallback of the device readout.
+void canonicalize_host(const std::vector<int64_t>& x, const std::vector<int64_t>& carries,
+                       const lnt_test* t, std::vector<uint64_t>& out) {
+  const uint32_t n = t->n;
+  std::vector<int64_t> v(x);
+  if (!carries.empty()) {
+    const lnt::Plan& P = t->plan;
+    for (uint32_t tt = 0; tt < P.ntiles; ++tt)
+      for (uint32_t r = 0; r < P.n2; ++r) {
+        // carry of run (tt, r) lands at the start of the next run
+        uint32_t nt = tt + 1, nr = r;
+        if (nt == P.ntiles) { nt = 0; nr = (r + 1) % P.n2; }
+        v[(size_t)nr * P.n1 + (size_t)nt * P.tile] += carries[(size_t)tt * P.n2 + r];
+      }
+  }
+  int64_t carry = 0;
+  uint32_t j = 0;
+  bool wrapped = false;
+  for (;;) {
+    int64_t s = v[j] + carry;
+    unsigned w = t->h_widths[j];
+    v[j] = s & ((int64_t(1) << w) - 1);
+    carry = s >> w;
+    if (++j == n) { j = 0; wrapped = true; }
+    if (wrapped && carry == 0) break;
+  }
+  out.assign(v.begin(), v.end());
+}
+
+// Apply the reference's choice between the two representations of 0 mod M:
+// LL residues are in [0, M-1]; PRP residues in [1, M] unless the test started
+// from an all-zero residue.
+void fix_zero_representation(const lnt_test* t, std::vector<uint64_t>& d) {
+  bool all_max = true, all_zero = true;
+  for (uint32_t j = 0; j < t->n; ++j) {
+    uint64_t mask = (1ull << t->h_widths[j]) - 1;
+    all_max &= d[j] == mask;
+    all_zero &= d[j] == 0;
+  }
+  if (!t->prp && all_max) std::fill(d.begin(), d.end(), 0);
+  if (t->prp && all_zero && !t->zero_start)
+    for (uint32_t j = 0; j < t->n; ++j) d[j] = (1ull << t->h_widths[j]) - 1;
+}
+
+int check_status(lnt_test* t) {
+  LNT_CUDA(cudaMemcpyAsync(t->h_pinned, t->status, 4, cudaMemcpyDeviceToHost, t->stream),
+           "read status");
+  LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
+  if (t->h_pinned[0] & lnt::kStatusCarryOverflow)
+    return fail(LNT_ERR_NUMERIC, "carry exceeded the balanced-digit headroom");
+  return LNT_OK;
+}
+
+// Bring `canon` up to date with the current residue.
+int canonicalize(lnt_test* t) {
+  if (t->canon_valid) return LNT_OK;
+  int st = check_status(t);
+  if (st != LNT_OK) return st;
+  if (t->pristine) {
+    LNT_CUDA(cudaMemcpyAsync(t->canon, t->x, (size_t)t->n * 8, cudaMemcpyDeviceToDevice, t->stream),
+             "copy digits");
+    LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
+    t->canon_valid = true;
+    return LNT_OK;
+  }
+  lnt::CanonDesc c{};
+  c.x = t->x;
+  c.carry = (t->plan.kind == lnt::PlanKind::TwoPass && t->pending_carries) ? t->carry : nullptr;
+  c.widths = t->widths;
+  c.out = t->canon;
+  c.blk_carry = t->blk_carry;
+  c.blk_fn = t->blk_fn;
+  c.blk_cin = t->blk_cin;
+  c.flags = t->cflags;
+  c.n = t->n;
+  c.block = lnt::canon_block_size(t->n);
+  c.nblocks = t->n / c.block;
+  c.n1 = t->plan.n1;
+  c.n2 = t->plan.n2;
+  c.tile = t->plan.tile;
+  c.ntiles = t->plan.ntiles;
+  LNT_CUDA(cudaMemsetAsync(t->cflags, 0, 4, t->stream), "memset flags");
+  LNT_CUDA(lnt::launch_canonicalize(c, t->stream), "canonical readout");
+  LNT_CUDA(cudaMemcpyAsync(t->h_pinned + 1, t->cflags, 4, cudaMemcpyDeviceToHost, t->stream),
+           "read flags");
+  LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
+  uint32_t flags = t->h_pinned[1];
+  if (flags & lnt::kCanonError) {
+    // host fallback: exact sequential carry
+    std::vector<int64_t> x(t->n), carries;
+    LNT_CUDA(cudaMemcpy(x.data(), t->x, (size_t)t->n * 8, cudaMemcpyDeviceToHost), "copy digits");
+    if (c.carry) {
+      carries.resize((size_t)t->plan.ntiles * t->plan.n2);
+      LNT_CUDA(cudaMemcpy(carries.data(), t->carry, carries.size() * 8, cudaMemcpyDeviceToHost),
+               "copy carries");
+    }
+    std::vector<uint64_t> out;
+    canonicalize_host(x, carries, t, out);
+    fix_zero_representation(t, out);
+    LNT_CUDA(cudaMemcpy(t->canon, out.data(), (size_t)t->n * 8, cudaMemcpyHostToDevice),
+             "upload digits");
+    t->canon_valid = true;
+    return LNT_OK;
+  }
+  const bool all_max = !(flags & lnt::kCanonNotAllMax);
+  if (!t->prp && all_max) {
+    LNT_CUDA(cudaMemsetAsync(t->canon, 0, (size_t)t->n * 8, t->stream), "zero residue");
+  } else if (t->prp && !t->zero_start && !(flags & lnt::kCanonHighNonZero)) {
+    uint64_t d0 = 0;
+    LNT_CUDA(cudaMemcpy(&d0, t->canon, 8, cudaMemcpyDeviceToHost), "read digit");
+    if (d0 == 0) LNT_CUDA(lnt::launch_fill_max(t->canon, t->widths, t->n, t->stream), "fill");
+  }
+  LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
+  t->canon_valid = true;
+  return LNT_OK;
+}
+
+int upload_digits(lnt_test* t, const uint64_t* digits) {
+  LNT_CUDA(cudaMemcpyAsync(t->x, digits, (size_t)t->n * 8, cudaMemcpyHostToDevice, t->stream),
+           "upload digits");
+  LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
+  bool zero = true;
+  for (uint32_t j = 0; j < t->n && zero; ++j) zero = digits[j] == 0;
+  t->zero_start = zero;
+  t->canonical_input = true;
+  t->pending_carries = false;
+  t->pristine = true;
+  t->canon_valid = false;
+  return LNT_OK;
+}
+
+// CUDA events recorded between kernel launches (lnt_profile_iterations).
+struct LaunchTimer {
+  std::vector<cudaEvent_t> events;
+  std::vector<const char*> kinds;  // kinds[i] ran between events[i] and events[i + 1]
+  ~LaunchTimer() {
+    for (cudaEvent_t e : events) cudaEventDestroy(e);
+  }
+  cudaError_t mark(cudaStream_t s) {
+    cudaEvent_t e;
+    cudaError_t r = cudaEventCreate(&e);
+    if (r != cudaSuccess) return r;
+    events.push_back(e);
+    return cudaEventRecord(e, s);
+  }
+};
+
+#define LNT_LAUNCH(call, kind)                                   \
+  do {                                                           \
+    if (timer && timer->events.empty())                          \
+      LNT_CUDA(timer->mark(t->stream), "event");                 \
+    LNT_CUDA(call, kind);                                        \
+    if (timer) {                                                 \
+      timer->kinds.push_back(kind);                              \
+      LNT_CUDA(timer->mark(t->stream), "event");                 \
+    }                                                            \
+  } while (0)
+
+// Queue `iterations` squarings on the test's stream (LucasPRP::MainLoop).
+int queue_iterations(lnt_test* t, uint64_t iterations, LaunchTimer* timer) {
+  if (t->plan.kind == lnt::PlanKind::Resident) {
+    lnt::ResidentDesc d{};
+    d.digits = t->x;
+    d.w = t->w;
+    d.uw = t->uw;
+    d.widths = t->widths;
+    d.rt = t->rt;
+    d.irt = t->irt;
+    d.status = t->status;
+    d.n = t->n;
+    d.log2n = t->plan.log2n;
+    d.prp = (uint32_t)t->prp;
+    d.unsigned_first = t->canonical_input ? 1 : 0;
+    d.iterations = iterations;
+    LNT_CUDA(cudaMemcpyAsync(t->rdesc, &d, sizeof(d), cudaMemcpyHostToDevice, t->stream),
+             "upload descriptor");
+    LNT_LAUNCH(lnt::launch_resident(t->rdesc, 1, t->n, t->stream), "resident_square_loop");
+    // the descriptor copy is staged from pageable memory: wait so `d` may go
+    LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
+  } else {
+    lnt::TwoPassDesc d = twopass_desc(t);
+    for (uint64_t i = 0; i < iterations; ++i) {
+      LNT_LAUNCH(lnt::launch_col_forward(d, t->pending_carries, t->stream), "col_forward");
+      LNT_LAUNCH(lnt::launch_row_square(d, t->stream), "row_square");
+      LNT_LAUNCH(lnt::launch_col_inverse(d, t->canonical_input, t->stream), "col_inverse");
+      t->pending_carries = true;
+      t->canonical_input = false;
+    }
+  }
+  t->canonical_input = false;
+  t->pristine = false;
+  t->canon_valid = false;
+  return LNT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* lnt_status_string(int status) {
+  switch (status) {
+    case LNT_OK: return "ok";
+    case LNT_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case LNT_ERR_UNSUPPORTED_LENGTH: return "unsupported NTT length";
+    case LNT_ERR_CUDA: return "CUDA error";
+    case LNT_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case LNT_ERR_NUMERIC: return "carry headroom exceeded";
+    case LNT_ERR_NO_DEVICE: return "no CUDA device";
+    case LNT_ERR_BUDGET: return "does not fit the memory budget";
+    default: return "unknown status";
+  }
+}
+
+const char* lnt_last_error(void) { return g_last_error.c_str(); }
+
+int lnt_create(uint32_t exponent, uint32_t n, int prp, int device, lnt_test** out) {
+  if (!out) return fail(LNT_ERR_INVALID_ARGUMENT, "null output pointer");
+  *out = nullptr;
+  if (exponent < 3) return fail(LNT_ERR_INVALID_ARGUMENT, "exponent must be >= 3");
+  if (n == 0) {
+    uint32_t l = lnt_secured_log2_length(exponent);
+    if (l < 1 || l > lnt::kMaxLog2) return fail(LNT_ERR_UNSUPPORTED_LENGTH, "exponent out of range");
+    n = 1u << l;
+  }
+  lnt::Plan plan;
+  if (!lnt::make_plan(n, plan)) return fail(LNT_ERR_UNSUPPORTED_LENGTH, "length must be 2^k, 1 <= k <= 26");
+  if (n > exponent) return fail(LNT_ERR_UNSUPPORTED_LENGTH, "length exceeds the exponent");
+  if ((exponent + n - 1) / n > 30) return fail(LNT_ERR_UNSUPPORTED_LENGTH, "more than 30 bits per word");
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+    return fail(LNT_ERR_NO_DEVICE, "no CUDA device");
+  if (device < 0 || device >= count) return fail(LNT_ERR_INVALID_ARGUMENT, "bad device index");
+  DeviceGuard guard(device);
+
+  lnt_test* t = new lnt_test();
+  t->q = exponent;
+  t->n = n;
+  t->prp = prp ? 1 : 0;
+  t->device = device;
+  t->plan = plan;
+  auto bail = [&](int st) {
+    free_all(t);
+    delete t;
+    return st;
+  };
+  cudaError_t e = cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return bail(cuda_fail(e, "cudaStreamCreate"));
+  t->own_stream = true;
+
+  // widths: ceil(q(j+1)/n) - ceil(qj/n) in double, as pre_calculation.cu:35
+  t->h_widths.resize(n);
+  for (uint32_t j = 0; j < n; ++j)
+    t->h_widths[j] = (uint8_t)(std::ceil(1.0 * exponent * (double)(j + 1) / n) -
+                               std::ceil(1.0 * exponent * (double)j / n));
+
+  const uint32_t cb = lnt::canon_block_size(n), nb = n / cb;
+  if ((e = dalloc(&t->x, n)) || (e = dalloc(&t->w, n)) || (e = dalloc(&t->uw, n)) ||
+      (e = dalloc(&t->widths, n)) || (e = dalloc(&t->status, 1)) || (e = dalloc(&t->canon, n)) ||
+      (e = dalloc(&t->blk_carry, nb)) || (e = dalloc(&t->blk_fn, nb)) ||
+      (e = dalloc(&t->blk_cin, nb)) || (e = dalloc(&t->cflags, 1)) ||
+      (e = cudaMallocHost((void**)&t->h_pinned, 16)))
+    return bail(cuda_fail(e, "allocate residue"));
+  if ((e = cudaMemcpy(t->widths, t->h_widths.data(), n, cudaMemcpyHostToDevice)) ||
+      (e = cudaMemset(t->status, 0, 4)))
+    return bail(cuda_fail(e, "upload widths"));
+  if ((e = lnt::launch_weights(exponent, n, t->w, t->uw, t->stream)))
+    return bail(cuda_fail(e, "weights"));
+
+  int st;
+  if (plan.kind == lnt::PlanKind::Resident) {
+    if ((st = upload_roots(t, n, &t->rt, &t->irt)) != LNT_OK) return bail(st);
+    if ((e = dalloc(&t->rdesc, 1))) return bail(cuda_fail(e, "allocate descriptor"));
+  } else {
+    if ((st = upload_roots(t, plan.n1, &t->rt1, &t->irt1)) != LNT_OK) return bail(st);
+    if ((st = upload_roots(t, plan.n2, &t->rt2, &t->irt2)) != LNT_OK) return bail(st);
+    if ((e = dalloc(&t->twf, n)) || (e = dalloc(&t->twi, n)) ||
+        (e = dalloc(&t->carry, (size_t)plan.ntiles * plan.n2)))
+      return bail(cuda_fail(e, "allocate twiddles"));
+    if ((e = lnt::launch_twiddles(plan.n1, plan.n2, plan.log2n2, t->twf, t->twi, t->stream)))
+      return bail(cuda_fail(e, "twiddles"));
+  }
+  if ((e = cudaStreamSynchronize(t->stream))) return bail(cuda_fail(e, "initialize"));
+  if ((st = lnt_init_test(t)) != LNT_OK) return bail(st);
+  *out = t;
+  return LNT_OK;
+}
+
+int lnt_destroy(lnt_test* t) {
+  if (!t) return LNT_OK;
+  DeviceGuard guard(t->device);
+  if (t->stream) cudaStreamSynchronize(t->stream);
+  free_all(t);
+  delete t;
+  return LNT_OK;
+}
+
+int lnt_init_test(lnt_test* t) {
+  if (!t) return fail(LNT_ERR_INVALID_ARGUMENT, "null test");
+  DeviceGuard guard(t->device);
+  std::vector<uint64_t> d(t->n, 0);
+  d[0] = t->prp ? 3 : 4;
+  return upload_digits(t, d.data());
+}
+
+int lnt_set_digits(lnt_test* t, const uint64_t* digits, size_t n) {
+  if (!t || !digits || n != t->n) return fail(LNT_ERR_INVALID_ARGUMENT, "digits/length mismatch");
+  DeviceGuard guard(t->device);
+  return upload_digits(t, digits);
+}
+
+int lnt_iterate(lnt_test* t, uint64_t iterations) {
+  if (!t) return fail(LNT_ERR_INVALID_ARGUMENT, "null test");
+  if (iterations == 0) return LNT_OK;
+  DeviceGuard guard(t->device);
+  return queue_iterations(t, iterations, nullptr);
+}
+
+int lnt_profile_iterations(lnt_test* t, uint64_t iterations, lnt_kernel_time* out, int cap,
+                           int* count) {
+  if (!t || !count || (cap > 0 && !out)) return fail(LNT_ERR_INVALID_ARGUMENT, "null argument");
+  DeviceGuard guard(t->device);
+  LaunchTimer timer;
+  int st = queue_iterations(t, iterations, &timer);
+  if (st != LNT_OK) return st;
+  LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
+  std::vector<lnt_kernel_time> kinds;
+  for (size_t i = 0; i < timer.kinds.size(); ++i) {
+    float ms = 0;
+    LNT_CUDA(cudaEventElapsedTime(&ms, timer.events[i], timer.events[i + 1]), "event time");
+    auto it = std::find_if(kinds.begin(), kinds.end(), [&](const lnt_kernel_time& k) {
+      return std::strcmp(k.name, timer.kinds[i]) == 0;
+    });
+    if (it == kinds.end()) {
+      lnt_kernel_time k{};
+      std::snprintf(k.name, sizeof(k.name), "%s", timer.kinds[i]);
+      kinds.push_back(k);
+      it = kinds.end() - 1;
+    }
+    it->launches++;
+    it->total_ms += ms;
+  }
+  *count = (int)kinds.size();
+  for (int i = 0; i < cap && i < (int)kinds.size(); ++i) out[i] = kinds[i];
+  return check_status(t);
+}
+
+int lnt_get_digits(lnt_test* t, uint64_t* digits, size_t n) {
+  if (!t || !digits || n != t->n) return fail(LNT_ERR_INVALID_ARGUMENT, "digits/length mismatch");
+  DeviceGuard guard(t->device);
+  int st = canonicalize(t);
+  if (st != LNT_OK) return st;
+  LNT_CUDA(cudaMemcpyAsync(digits, t->canon, (size_t)t->n * 8, cudaMemcpyDeviceToHost, t->stream),
+           "download digits");
+  LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
+  return LNT_OK;
+}
+
+int lnt_res64(lnt_test* t, uint64_t* res64) {
+  if (!t || !res64) return fail(LNT_ERR_INVALID_ARGUMENT, "null argument");
+  DeviceGuard guard(t->device);
+  int st = canonicalize(t);
+  if (st != LNT_OK) return st;
+  uint64_t head[64];
+  const uint32_t k = t->n < 64 ? t->n : 64;
+  LNT_CUDA(cudaMemcpy(head, t->canon, k * 8, cudaMemcpyDeviceToHost), "download digits");
+  uint64_t r = 0;
+  uint32_t pos = 0;
+  for (uint32_t j = 0; j < k && pos < 64; ++j) {
+    r += head[j] << pos;
+    pos += t->h_widths[j];
+  }
+  *res64 = r;
+  return LNT_OK;
+}
+
+int lnt_is_prime(lnt_test* t, int* is_prime) {
+  if (!t || !is_prime) return fail(LNT_ERR_INVALID_ARGUMENT, "null argument");
+  DeviceGuard guard(t->device);
+  std::vector<uint64_t> d(t->n);
+  int st = lnt_get_digits(t, d.data(), d.size());
+  if (st != LNT_OK) return st;
+  bool prime = d[0] == (uint64_t)(t->prp ? 9 : 0);
+  for (uint32_t j = 1; j < t->n && prime; ++j) prime = d[j] == 0;
+  *is_prime = prime ? 1 : 0;
+  return LNT_OK;
+}
+
+int lnt_get_raw_state(lnt_test* t, int64_t* words, size_t n) {
+  if (!t || !words || n != t->n) return fail(LNT_ERR_INVALID_ARGUMENT, "words/length mismatch");
+  DeviceGuard guard(t->device);
+  LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
+  LNT_CUDA(cudaMemcpy(words, t->x, (size_t)t->n * 8, cudaMemcpyDeviceToHost), "download state");
+  return LNT_OK;
+}
+
+int lnt_get_length(lnt_test* t, uint32_t* n) {
+  if (!t || !n) return fail(LNT_ERR_INVALID_ARGUMENT, "null argument");
+  *n = t->n;
+  return LNT_OK;
+}
+
+int lnt_get_widths(lnt_test* t, uint8_t* widths, size_t n) {
+  if (!t || !widths || n != t->n) return fail(LNT_ERR_INVALID_ARGUMENT, "widths/length mismatch");
+  std::memcpy(widths, t->h_widths.data(), n);
+  return LNT_OK;
+}
+
+int lnt_plan_name(lnt_test* t, char* out, size_t outlen) {
+  if (!t || !out || outlen == 0) return fail(LNT_ERR_INVALID_ARGUMENT, "null argument");
+  std::snprintf(out, outlen, "%s", t->plan.name.c_str());
+  return LNT_OK;
+}
+
+int lnt_set_stream(lnt_test* t, void* cuda_stream) {
+  if (!t) return fail(LNT_ERR_INVALID_ARGUMENT, "null test");
+  DeviceGuard guard(t->device);
+  LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
+  if (cuda_stream) {
+    if (t->own_stream) cudaStreamDestroy(t->stream);
+    t->stream = (cudaStream_t)cuda_stream;
+    t->own_stream = false;
+  } else if (!t->own_stream) {
+    LNT_CUDA(cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    t->own_stream = true;
+  }
+  return LNT_OK;
+}
+
+int lnt_synchronize(lnt_test* t) {
+  if (!t) return fail(LNT_ERR_INVALID_ARGUMENT, "null test");
+  DeviceGuard guard(t->device);
+  return check_status(t);
+}
+
+}  // extern "C"

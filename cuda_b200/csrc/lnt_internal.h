@@ -1,0 +1,112 @@
+// Internal declarations of the LucasNTT B200 library: plan, kernel descriptors
+// and launchers.  Nothing here is part of the C ABI (include/lucasntt.h).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+
+namespace lnt {
+
+// Status bits a kernel may raise in its status word.
+enum : uint32_t {
+  kStatusCarryOverflow = 1u << 0,  // a run absorbed a carry above kAbsorbLimit
+  kStatusCanonFallback = 1u << 1,  // canonical readout needs the host fallback
+};
+
+// ---------------------------------------------------------------- plans ----
+// How one squaring of an n-word residue is laid out on the GPU.  Replaces the
+// reference's pool/length choice (kernel_pool.cu:17-142, lucas_prp.cu:36-70).
+enum class PlanKind { Resident, TwoPass };
+
+struct Plan {
+  PlanKind kind = PlanKind::Resident;
+  uint32_t n = 0, log2n = 0;
+  // TwoPass: natural index j = j1 + n1 * j2 is stored row-major (row j2,
+  // column j1).  Columns (stride n1, length n2) are transformed by the column
+  // passes, rows (contiguous, length n1) by the row pass.
+  uint32_t n1 = 0, n2 = 0, log2n1 = 0, log2n2 = 0;
+  uint32_t tile = 0;    // columns per column-pass CTA = words per carry run
+  uint32_t ntiles = 0;  // n1 / tile
+  std::string name;
+};
+
+// Largest length handled by the SMEM-resident single-CTA kernel.
+constexpr uint32_t kResidentMaxLog2 = 12;
+constexpr uint32_t kMaxLog2 = 26;  // (p - 1) / 192 holds 2^26: the largest IBDWT length
+
+bool make_plan(uint32_t n, Plan& plan);
+
+// ------------------------------------------------------ resident kernel ----
+// One residue per CTA, state kept in shared memory for all iterations.
+struct ResidentDesc {
+  int64_t* digits;        // n words, natural order (balanced or canonical)
+  const uint64_t* w;      // IBDWT weights
+  const uint64_t* uw;     // unweights with 1/n folded in
+  const uint8_t* widths;  // digit widths
+  const uint64_t* rt;     // omega_n^k, k < n/2
+  const uint64_t* irt;    // omega_n^-k
+  uint32_t* status;
+  uint32_t n, log2n;
+  uint32_t prp;
+  uint32_t unsigned_first;  // the first squaring reads its outputs as non-negative
+  uint64_t iterations;      // squarings this CTA performs in the launch
+};
+
+size_t resident_smem_bytes(uint32_t n, uint32_t threads);
+uint32_t resident_threads(uint32_t n);
+cudaError_t launch_resident(const ResidentDesc* d_descs, uint32_t count, uint32_t max_n,
+                            cudaStream_t stream);
+
+// ------------------------------------------------------ two-pass kernels ----
+struct TwoPassDesc {
+  int64_t* x;             // n words: digits, or the column-transformed residue
+  int64_t* carry;         // pending run carries, index tile * n2 + row
+  const uint64_t* w;
+  const uint64_t* uw;
+  const uint8_t* widths;
+  const uint64_t* twf;    // 4-step twiddles omega_n^(j1 * brev(row)), n2 x n1
+  const uint64_t* twi;    // their inverses
+  const uint64_t* rt1;    // row roots omega_n1^k, k < n1/2
+  const uint64_t* irt1;
+  const uint64_t* rt2;    // column roots omega_n2^k, k < n2/2
+  const uint64_t* irt2;
+  uint32_t* status;
+  uint32_t n1, n2, log2n1, log2n2, tile, ntiles;
+  uint32_t prp;
+};
+
+cudaError_t launch_col_forward(const TwoPassDesc& d, bool apply_carries, cudaStream_t s);
+cudaError_t launch_row_square(const TwoPassDesc& d, cudaStream_t s);
+cudaError_t launch_col_inverse(const TwoPassDesc& d, bool unsigned_mode, cudaStream_t s);
+
+// ------------------------------------------------------------- tables ----
+cudaError_t launch_weights(uint32_t exponent, uint32_t n, uint64_t* w, uint64_t* uw,
+                           cudaStream_t s);
+cudaError_t launch_twiddles(uint32_t n1, uint32_t n2, uint32_t log2n2, uint64_t* twf,
+                            uint64_t* twi, cudaStream_t s);
+
+// --------------------------------------------------- canonical readout ----
+struct CanonDesc {
+  const int64_t* x;        // balanced digits
+  const int64_t* carry;    // pending run carries or nullptr
+  const uint8_t* widths;
+  uint64_t* out;           // canonical non-negative digits
+  int64_t* blk_carry;      // per block
+  uint8_t* blk_fn;         // per block carry transfer function
+  int8_t* blk_cin;         // per block resolved carry-in
+  uint32_t* flags;         // kCanon* bits
+  uint32_t n, block, nblocks;
+  uint32_t n1, n2, tile, ntiles;  // run geometry when carry != nullptr
+};
+
+enum : uint32_t {
+  kCanonNotAllMax = 1u << 0,
+  kCanonHighNonZero = 1u << 1,  // some digit j >= 1 is non-zero
+  kCanonError = 1u << 2,        // needs the host fallback
+};
+
+uint32_t canon_block_size(uint32_t n);
+cudaError_t launch_canonicalize(const CanonDesc& d, cudaStream_t s);
+cudaError_t launch_fill_max(uint64_t* out, const uint8_t* widths, uint32_t n, cudaStream_t s);
+
+}  // namespace lnt

@@ -1,0 +1,66 @@
+// Precomputed tables: IBDWT weights/unweights and 4-step twiddles.
+//
+// Replaces common/pre_calculation.cu:23-36 (calc_weights_widths) and :69-77
+// (calc_brev_factors).  The weights are the same field elements as the
+// reference's: w_j = 7^(((p-1)/192/n) * 5 * (n - r_j)), r_j = q j mod n, w_0 = 1,
+// uw_j = (w_j n)^-1, uw_0 = n^-1.  With g = 7^(((p-1)/192/n) * 5) (g^n = 2),
+// uw_j = g^r_j / (2n) for j > 0.  Widths are computed on the host with the
+// reference's double-precision expression.
+#include "lnt_internal.h"
+#include "goldilocks.cuh"
+
+namespace lnt {
+
+namespace {
+
+__global__ void weights_kernel(uint32_t exponent, uint32_t n, uint64_t g, uint64_t inv_n,
+                               uint64_t inv_2n, uint64_t* w, uint64_t* uw) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  if (j == 0) {
+    w[0] = 1;
+    uw[0] = inv_n;
+    return;
+  }
+  const uint32_t r = (exponent * j) & (n - 1);  // 32-bit product: only the low bits matter
+  w[j] = gl::pow(g, (uint64_t)(n - r));
+  uw[j] = gl::mul(gl::pow(g, (uint64_t)r), inv_2n);
+}
+
+// twf[row * n1 + j1] = omega_n^(j1 * k2) with k2 = bit-reverse(row) over log2n2
+// bits: the frequency that the forward column NTT leaves in memory row `row`.
+__global__ void twiddle_kernel(uint32_t n1, uint32_t n2, uint32_t log2n2, uint64_t root,
+                               uint64_t iroot, uint64_t* twf, uint64_t* twi) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (size_t)n1 * n2) return;
+  const uint32_t row = (uint32_t)(idx / n1), j1 = (uint32_t)(idx % n1);
+  const uint32_t k2 = __brev(row) >> (32 - log2n2);
+  const uint64_t e = (uint64_t)j1 * k2;
+  twf[idx] = gl::pow(root, e);
+  twi[idx] = gl::pow(iroot, e);
+}
+
+}  // namespace
+
+cudaError_t launch_weights(uint32_t exponent, uint32_t n, uint64_t* w, uint64_t* uw,
+                           cudaStream_t s) {
+  const uint64_t c = ((gl::P - 1) / 192 / n) * 5ull;
+  const uint64_t g = gl::pow(7, c);
+  const uint64_t inv_n = gl::inv(n), inv_2n = gl::inv(2ull * n);
+  const uint32_t threads = 256, blocks = (n + threads - 1) / threads;
+  weights_kernel<<<blocks, threads, 0, s>>>(exponent, n, g, inv_n, inv_2n, w, uw);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_twiddles(uint32_t n1, uint32_t n2, uint32_t log2n2, uint64_t* twf,
+                            uint64_t* twi, cudaStream_t s) {
+  const uint64_t n = (uint64_t)n1 * n2;
+  const uint64_t root = gl::pow(554, (gl::P - 1) / n);
+  const uint64_t iroot = gl::inv(root);
+  const uint32_t threads = 256;
+  const uint64_t blocks = (n + threads - 1) / threads;
+  twiddle_kernel<<<(unsigned)blocks, threads, 0, s>>>(n1, n2, log2n2, root, iroot, twf, twi);
+  return cudaGetLastError();
+}
+
+}  // namespace lnt

@@ -1,0 +1,139 @@
+/*
+ * lucasntt.h -- C ABI of the B200 LucasNTT squaring loop (liblucasntt.so).
+ *
+ * The reference LucasNTT program is a monolithic binary with no plugin or FFI;
+ * its internal seam for this path is the Process interface
+ * (process.cuh:16-35) implemented by LucasPRP (lucas_prp.cu) over a KernelPool
+ * (kernel_pool.cu), with the length policy in NttLengths (ntt_lengths.cu).
+ * Each entry point below names the reference function it replaces.
+ *
+ * Conventions: plain C types only; every call returns an lnt_status (0 = ok)
+ * and never throws; the context owns its device memory.  Digits are the
+ * reference's residue words: one uint64 per word, natural order, each word
+ * d_j in [0, 2^w_j) with w_j = ceil(q(j+1)/n) - ceil(qj/n), exactly the vector
+ * the reference dumps to LucasNTT_results.dat (lucas_prp.cu:254-263).
+ */
+#ifndef LUCASNTT_H
+#define LUCASNTT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum lnt_status {
+  LNT_OK = 0,
+  LNT_ERR_INVALID_ARGUMENT = 1, /* bad pointer, size or exponent */
+  LNT_ERR_UNSUPPORTED_LENGTH = 2, /* n not a power of two in [2, 2^26] or n > q */
+  LNT_ERR_CUDA = 3,             /* a CUDA call failed; see lnt_last_error() */
+  LNT_ERR_OUT_OF_MEMORY = 4,    /* device allocation failed */
+  LNT_ERR_NUMERIC = 5,          /* carry headroom exceeded: the residue is not trustworthy */
+  LNT_ERR_NO_DEVICE = 6,        /* no CUDA device */
+  LNT_ERR_BUDGET = 7            /* batch/serving: request does not fit the HBM budget */
+} lnt_status;
+
+typedef struct lnt_test lnt_test;
+
+/* Text of a status code. */
+const char* lnt_status_string(int status);
+
+/* Detail of the last failure on the calling thread ("" if none). */
+const char* lnt_last_error(void);
+
+/* ---- length policy --------------------------------------------------------- */
+
+/* NttLengths::GetNttSecuredLength (ntt_lengths.cu:88-98): log2 of the NTT
+ * length the reference picks for exponent q. */
+uint32_t lnt_secured_log2_length(uint32_t exponent);
+
+/* NttLengths::GetCandidates (ntt_lengths.cu:100-128): writes the candidate
+ * length strings, ';'-terminated, exactly as the reference spells them
+ * ("8388608.000000;2048.000000:4096.000000;..."). Returns the count. */
+int lnt_length_candidates(uint32_t exponent, char* out, size_t outlen);
+
+/* NttLengths::StringToLengths + GetTotalLength (ntt_lengths.cu:32-75,
+ * :130-142): total length of an "fft" description such as "4096", "8M",
+ * "2048:4096".  Returns LNT_ERR_INVALID_ARGUMENT for lengths the reference
+ * rejects (factors other than 2, 3, 5) and LNT_ERR_UNSUPPORTED_LENGTH for
+ * non-power-of-two totals (the reference has no kernel for those either). */
+int lnt_parse_length(const char* description, uint32_t* n_out);
+
+/* NttLengths::CheckProvidedLength (ntt_lengths.cu:77-86): secured log2 length
+ * minus log2 of the provided description (> 0: too small, < 0: larger than
+ * needed).  Writes the difference to *diff. */
+int lnt_check_provided_length(uint32_t exponent, const char* description, int* diff);
+
+/* ---- one test ---------------------------------------------------------------- */
+
+/* LucasPRP::LucasPRP + LucasPRP::Initialize (lucas_prp.cu:24-72, :82-111):
+ * allocate the residue and its tables for exponent q on CUDA device `device`,
+ * NTT length n (0 = the reference's policy), PRP (prp != 0) or Lucas-Lehmer,
+ * and set the start value (InitializeTest, lucas_prp.cu:127-134). */
+int lnt_create(uint32_t exponent, uint32_t n, int prp, int device, lnt_test** out);
+
+/* LucasPRP::Finalize + ~LucasPRP (lucas_prp.cu:113-125, :74-80). NULL is ok. */
+int lnt_destroy(lnt_test* t);
+
+/* LucasPRP::InitializeTest (lucas_prp.cu:127-134): residue := 4 (LL) or 3 (PRP). */
+int lnt_init_test(lnt_test* t);
+
+/* LucasPRP::MainLoop / OneIteration (lucas_prp.cu:197-229): `iterations`
+ * squarings, each followed by minus two for LL.  Asynchronous on the test's
+ * stream; errors raised by the kernels are reported by the next readout. */
+int lnt_iterate(lnt_test* t, uint64_t iterations);
+
+/* LucasPRP::LoadResidue (lucas_prp.cu:326-346): replace the residue with the
+ * n digits at `digits` (host memory, natural order, as dumped). */
+int lnt_set_digits(lnt_test* t, const uint64_t* digits, size_t n);
+
+/* The device-to-host copy of lucas_prp.cu:164 + DumpResidue's word order
+ * (lucas_prp.cu:254-263): write the residue's n digits to host memory. */
+int lnt_get_digits(lnt_test* t, uint64_t* digits, size_t n);
+
+/* Low 64 bits of the residue value sum d_j 2^ceil(qj/n) (Res64, derived from
+ * the dumped digits; the reference prints no Res64 itself). */
+int lnt_res64(lnt_test* t, uint64_t* res64);
+
+/* Verdict of LucasPRP::Run (lucas_prp.cu:167-184): *is_prime = 1 when the
+ * residue is 0 (LL) or 9 (PRP). Meaningful after the full test. */
+int lnt_is_prime(lnt_test* t, int* is_prime);
+
+/* Length, widths (n bytes, pre_calculation.cu:35) and plan name of a test. */
+int lnt_get_length(lnt_test* t, uint32_t* n);
+int lnt_get_widths(lnt_test* t, uint8_t* widths, size_t n);
+int lnt_plan_name(lnt_test* t, char* out, size_t outlen);
+
+/* Run the test's work on a caller-owned cudaStream_t (NULL = the test's own
+ * stream), the analogue of common::stream (common/common.cu:118). */
+int lnt_set_stream(lnt_test* t, void* cuda_stream);
+
+/* Wait for queued work; reports kernel-raised errors (LNT_ERR_NUMERIC). */
+int lnt_synchronize(lnt_test* t);
+
+/* Diagnostic without a reference counterpart: the internal representation,
+ * n signed words (balanced digits, or the reference's digits right after a
+ * set), before pending carries are applied and before canonicalisation. */
+int lnt_get_raw_state(lnt_test* t, int64_t* words, size_t n);
+
+/* Per-kernel device time of a run of squarings. */
+typedef struct lnt_kernel_time {
+  char name[32];     /* kernel kind, e.g. "col_forward" */
+  uint32_t launches; /* launches of that kind */
+  float total_ms;    /* summed CUDA-event time of those launches */
+} lnt_kernel_time;
+
+/* Process::EvaluatePerformance (process.cu:133-149), which times a candidate
+ * with cudaEvents: performs `iterations` squarings exactly as lnt_iterate, with
+ * a CUDA event recorded on the test's stream between consecutive kernel
+ * launches, then waits and writes up to `cap` per-kind totals to `out`
+ * (count in *count).  The residue advances as with lnt_iterate. */
+int lnt_profile_iterations(lnt_test* t, uint64_t iterations, lnt_kernel_time* out, int cap,
+                           int* count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LUCASNTT_H */

@@ -1,0 +1,149 @@
+"""GPU parity: the CUDA path (through the C ABI) against the oracle.
+
+Bar: bit-exact digits.  Small sizes compare every digit with the CPU oracle
+(oracle/lnt_oracle.c) or the big-integer fixture; full sizes compare Res64
+with committed fixtures and use size-independent properties (split
+iterations, set/get round trips, canonical digit ranges).
+"""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import bigint_model as B
+
+pytestmark = pytest.mark.gpu
+GOLDEN = Path(__file__).resolve().parent / "golden"
+MERSENNE = [89, 107, 127, 521, 607, 1279, 2203, 2281, 3217, 4253, 4423, 9689, 9941, 11213]
+
+
+def random_digits(q, n, seed):
+    rng = np.random.default_rng(seed)
+    w = np.array(B.widths(q, n), dtype=np.uint64)
+    return (rng.integers(0, 2**62, size=n, dtype=np.uint64) % (np.uint64(1) << w)).astype(np.uint64)
+
+
+def compare_with_oracle(lnt, oracle_mod, q, n, prp, iterations, start=None, steps=None):
+    with lnt.LucasTest(q, n, prp) as G, oracle_mod.OracleTest(q, n, prp) as O:
+        if start is not None:
+            G.set_digits(start)
+            O.set_digits(start)
+        for k in (steps or [iterations]):
+            G.iterate(k)
+            O.iterate(k)
+        g, o = G.digits(), O.digits()
+        bad = np.nonzero(g != o)[0]
+        assert bad.size == 0, f"q={q} n={n} prp={prp} first mismatch at {bad[:5]}: {g[bad[:5]]} vs {o[bad[:5]]}"
+        assert G.res64() == O.res64()
+        return G.plan
+
+
+@pytest.mark.parametrize("q", MERSENNE)
+def test_known_primes_resident(lnt, q):
+    with lnt.LucasTest(q, prp=False) as T:
+        T.iterate(q - 2)
+        assert T.is_prime() and T.res64() == 0
+    with lnt.LucasTest(q, prp=True) as T:
+        T.iterate(q)
+        assert T.is_prime() and T.res64() == 9
+
+
+def test_bigint_fixture(lnt):
+    cases = json.loads((GOLDEN / "small_bigint.json").read_text())["cases"]
+    for c in cases:
+        with lnt.LucasTest(c["q"], c["n"], c["prp"]) as T:
+            T.iterate(c["iterations"])
+            assert f"{T.res64():016x}" == c["res64"], c
+            assert T.digits()[:4].tolist() == c["digits_head"], c
+
+
+@pytest.mark.parametrize("q,n", [(89, 4), (127, 8), (1009, 64), (9973, 512), (44497, 2048),
+                                 (44497, 4096), (53239, 2048), (100003, 4096)])
+@pytest.mark.parametrize("prp", [False, True])
+def test_resident_random_state(lnt, oracle_mod, q, n, prp):
+    """Random canonical digits at the top of their range, several squarings."""
+    plan = compare_with_oracle(lnt, oracle_mod, q, n, prp, 0, start=random_digits(q, n, q + n),
+                               steps=[1, 4])
+    assert plan.startswith("RESIDENT")
+
+
+@pytest.mark.parametrize("q,n", [(160001, 8192), (300007, 16384), (1000003, 65536),
+                                 (2000003, 131072), (5000011, 262144), (20000003, 1 << 20)])
+def test_twopass_random_state(lnt, oracle_mod, q, n):
+    plan = compare_with_oracle(lnt, oracle_mod, q, n, False, 0, start=random_digits(q, n, q),
+                               steps=[1, 2])
+    assert plan.startswith("TWOPASS")
+
+
+@pytest.mark.parametrize("prp", [False, True])
+def test_twopass_from_start_value(lnt, oracle_mod, prp):
+    compare_with_oracle(lnt, oracle_mod, 160001, 8192, prp, 0, steps=[1, 1, 30])
+
+
+def test_c2_first_iterations(lnt, oracle_mod):
+    """q = 139000003 at the reference's length 2^23: bit-exact after 2 squarings."""
+    compare_with_oracle(lnt, oracle_mod, 139000003, 1 << 23, False, 0, steps=[1, 1])
+
+
+def test_c2_res64_fixture(lnt):
+    path = GOLDEN / "c2_oracle.json"
+    if not path.exists():
+        pytest.skip("c2 fixture not generated")
+    fx = json.loads(path.read_text())
+    with lnt.LucasTest(fx["q"], fx["n"], False) as T:
+        done = 0
+        for mark in sorted(int(k) for k in fx["res64_after"]):
+            T.iterate(mark - done)
+            done = mark
+            assert f"{T.res64():016x}" == fx["res64_after"][str(mark)], mark
+
+
+def test_c1_full_tests(lnt):
+    path = GOLDEN / "c1_oracle.json"
+    if not path.exists():
+        pytest.skip("c1 fixture not generated")
+    for c in json.loads(path.read_text())["cases"]:
+        with lnt.LucasTest(c["q"], c["n"], False) as T:
+            T.iterate(c["iterations"])
+            assert f"{T.res64():016x}" == c["res64"], c
+            assert T.is_prime() == c["is_prime"], c
+
+
+@pytest.mark.parametrize("q,n", [(1009, 64), (44497, 2048), (160001, 8192)])
+def test_split_iterations_equal_one_call(lnt, q, n):
+    with lnt.LucasTest(q, n) as A, lnt.LucasTest(q, n) as Bt:
+        A.iterate(37)
+        for k in (1, 5, 10, 21):
+            Bt.iterate(k)
+        assert np.array_equal(A.digits(), Bt.digits())
+
+
+@pytest.mark.parametrize("q,n", [(1009, 64), (160001, 8192)])
+def test_set_get_round_trip(lnt, q, n):
+    d = random_digits(q, n, 7)
+    with lnt.LucasTest(q, n) as T:
+        T.set_digits(d)
+        assert np.array_equal(T.digits(), d)
+        T.iterate(3)
+        out = T.digits()
+        assert np.all(out < (np.uint64(1) << T.widths().astype(np.uint64)))
+
+
+@pytest.mark.parametrize("q,n", [(1009, 64), (4099, 256), (160001, 8192)])
+@pytest.mark.parametrize("prp", [False, True])
+def test_zero_and_full_residues(lnt, oracle_mod, q, n, prp):
+    """All-zero and all-full (= M) starts exercise the 0 / M choice and the
+    long borrow chains of the canonical readout."""
+    widths = B.widths(q, n)
+    full = np.array([(1 << w) - 1 for w in widths], dtype=np.uint64)
+    for start in (np.zeros(n, np.uint64), full):
+        compare_with_oracle(lnt, oracle_mod, q, n, prp, 0, start=start, steps=[1, 2])
+
+
+def test_two_pass_known_prime(lnt):
+    """M_132049 is prime; its length 8192 runs on the two-pass plan."""
+    with lnt.LucasTest(132049, prp=False) as T:
+        assert T.plan.startswith("TWOPASS")
+        T.iterate(132049 - 2)
+        assert T.is_prime()

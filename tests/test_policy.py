@@ -1,0 +1,51 @@
+"""CPU: the library's length policy equals the reference's (ntt_lengths.cu:32-128)."""
+import random
+
+import pytest
+
+from oracle import oracle as O
+
+
+def test_secured_length_matches_oracle(lnt):
+    rng = random.Random(5)
+    qs = [33, 64, 89, 1000, 44497, 53248, 53249, 65536, 100000, 2000000, 5000000,
+          20000000, 30000000, 139000003, 1 << 30, 2**31 - 1]
+    qs += [rng.randrange(40, 2**31) for _ in range(2000)]
+    for q in qs:
+        assert lnt.secured_log2_length(q) == O.secured_log2(q), q
+
+
+@pytest.mark.parametrize("q,log2n", [(44497, 11), (139000003, 23), (100000, 12), (2000000, 17),
+                                     (5000000, 18), (20000000, 20), (10000, 9), (30000000, 21)])
+def test_config_lengths(lnt, q, log2n):
+    assert lnt.secured_log2_length(q) == log2n
+
+
+def test_candidate_strings(lnt):
+    for q in (44497, 139000003, 300000000, 600000000, 1100000000, 1000):
+        assert lnt.length_candidates(q) == O.candidates(q)
+    assert lnt.length_candidates(139000003) == [
+        "8388608.000000", "2048.000000:4096.000000", "4096.000000:2048.000000",
+        "256:256:128", "512:256:64"]
+
+
+def test_parse_length(lnt):
+    assert lnt.parse_length("4096") == 4096
+    assert lnt.parse_length("8M") == 1 << 23
+    assert lnt.parse_length("4K") == 4096
+    assert lnt.parse_length("2048:4096") == 1 << 23
+    assert lnt.parse_length("2048.000000:4096.000000") == 1 << 23
+    with pytest.raises(lnt.LucasNTTError) as e:
+        lnt.parse_length("3072")  # 3 * 2^10: valid in the reference, no kernel for it
+    assert e.value.status == 2
+    for bad in ("7", "9", "", "abc", "25"):
+        with pytest.raises(lnt.LucasNTTError) as e:
+            lnt.parse_length(bad)
+        assert e.value.status == 1
+
+
+def test_check_provided_length(lnt):
+    assert lnt.check_provided_length(44497, "2048") == 0
+    assert lnt.check_provided_length(44497, "4096") == -1
+    assert lnt.check_provided_length(44497, "1024") == 1
+    assert lnt.check_provided_length(139000003, "2048:4096") == 0
