@@ -344,6 +344,11 @@ int queue_iterations(lnt_test* t, uint64_t iterations, LaunchTimer* timer) {
 
 }  // namespace
 
+namespace lnt {
+// Lets other translation units of the library report a failure detail.
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace lnt
+
 extern "C" {
 
 const char* lnt_status_string(int status) {

@@ -132,6 +132,26 @@ typedef struct lnt_kernel_time {
 int lnt_profile_iterations(lnt_test* t, uint64_t iterations, lnt_kernel_time* out, int cap,
                            int* count);
 
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory when they need a residue in the reference's digit format (a serving
+ * process whose HBM is all handed to its own pool or budget, a latency-critical
+ * step that must not pay cudaMalloc's implicit device synchronisation, a
+ * checkpoint taken from an interrupt handler): turns n signed words `words`
+ * (balanced or non-negative digits of a residue, widths `widths`) into the
+ * reference's canonical digits, written to `digits`.  All three are DEVICE
+ * pointers owned by the caller; nothing is allocated.  The scratch lives in one
+ * library-owned array of device memory sized for n <= 2^24 (about 2.5 MiB, held
+ * by every GPU that loads the library until exit); larger n is rejected with
+ * LNT_ERR_INVALID_ARGUMENT.  prp / zero_start select the reference's
+ * representation of 0 mod M (LL: 0; PRP: M unless the test started from zero).
+ * The first call on a device sets up the scratch address, so make it before
+ * any stream capture.  Every call shares the one array: calls that overlap on
+ * the GPU (other streams, other threads) race.  Runs on `cuda_stream` (NULL =
+ * legacy default stream) and returns after it finished (LNT_ERR_NUMERIC if
+ * the words were too far from normalised digits). */
+int lnt_canonicalize_noalloc(const int64_t* words, const uint8_t* widths, uint32_t n, int prp,
+                             int zero_start, uint64_t* digits, void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif
