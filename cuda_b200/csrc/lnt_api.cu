@@ -38,6 +38,7 @@ struct lnt_test {
   // two-pass plan
   uint64_t *twf = nullptr, *twi = nullptr;
   uint64_t *rt1 = nullptr, *irt1 = nullptr, *rt2 = nullptr, *irt2 = nullptr;
+  uint64_t *itw1 = nullptr, *iitw1 = nullptr, *itw2 = nullptr, *iitw2 = nullptr;
   int64_t* carry = nullptr;
   // canonical readout
   uint64_t* canon = nullptr;
@@ -94,7 +95,8 @@ cudaError_t dalloc(T** p, size_t count) {
 
 void free_all(lnt_test* t) {
   void* ptrs[] = {t->x, t->w, t->uw, t->widths, t->status, t->rt, t->irt, t->rdesc,
-                  t->twf, t->twi, t->rt1, t->irt1, t->rt2, t->irt2, t->carry, t->canon,
+                  t->twf, t->twi, t->rt1, t->irt1, t->rt2, t->irt2, t->itw1, t->iitw1,
+                  t->itw2, t->iitw2, t->carry, t->canon,
                   t->blk_carry, t->blk_fn, t->blk_cin, t->cflags};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -112,10 +114,25 @@ void root_table(uint32_t n, bool inverse, std::vector<uint64_t>& out) {
   for (size_t k = 1; k < half; ++k) out[k] = gl::mul(out[k - 1], r);
 }
 
-int upload_roots(lnt_test* t, uint32_t n, uint64_t** rt, uint64_t** irt) {
+// omega_n^e for all e < n (the fast kernels index it with i1 * k2 < n).
+void power_table(uint32_t n, bool inverse, std::vector<uint64_t>& out) {
+  uint64_t r = gl::pow(554, (gl::P - 1) / n);
+  if (inverse) r = gl::inv(r);
+  out.resize(n);
+  out[0] = 1;
+  for (size_t k = 1; k < n; ++k) out[k] = gl::mul(out[k - 1], r);
+}
+
+// full = false: root_table (n/2 entries); full = true: power_table (n entries)
+int upload_roots(lnt_test* t, uint32_t n, uint64_t** rt, uint64_t** irt, bool full = false) {
   std::vector<uint64_t> a, b;
-  root_table(n, false, a);
-  root_table(n, true, b);
+  if (full) {
+    power_table(n, false, a);
+    power_table(n, true, b);
+  } else {
+    root_table(n, false, a);
+    root_table(n, true, b);
+  }
   LNT_CUDA(dalloc(rt, a.size()), "cudaMalloc roots");
   LNT_CUDA(dalloc(irt, b.size()), "cudaMalloc roots");
   LNT_CUDA(cudaMemcpy(*rt, a.data(), a.size() * 8, cudaMemcpyHostToDevice), "copy roots");
@@ -136,6 +153,10 @@ lnt::TwoPassDesc twopass_desc(const lnt_test* t) {
   d.irt1 = t->irt1;
   d.rt2 = t->rt2;
   d.irt2 = t->irt2;
+  d.itw1 = t->itw1;
+  d.iitw1 = t->iitw1;
+  d.itw2 = t->itw2;
+  d.iitw2 = t->iitw2;
   d.status = t->status;
   d.n1 = t->plan.n1;
   d.n2 = t->plan.n2;
@@ -329,9 +350,15 @@ int queue_iterations(lnt_test* t, uint64_t iterations, LaunchTimer* timer) {
   } else {
     lnt::TwoPassDesc d = twopass_desc(t);
     for (uint64_t i = 0; i < iterations; ++i) {
-      LNT_LAUNCH(lnt::launch_col_forward(d, t->pending_carries, t->stream), "col_forward");
-      LNT_LAUNCH(lnt::launch_row_square(d, t->stream), "row_square");
-      LNT_LAUNCH(lnt::launch_col_inverse(d, t->canonical_input, t->stream), "col_inverse");
+      if (t->plan.fast) {
+        LNT_LAUNCH(lnt::launch_col_forward_fast(d, t->pending_carries, t->stream), "col_forward");
+        LNT_LAUNCH(lnt::launch_row_square_fast(d, t->stream), "row_square");
+        LNT_LAUNCH(lnt::launch_col_inverse_fast(d, t->canonical_input, t->stream), "col_inverse");
+      } else {
+        LNT_LAUNCH(lnt::launch_col_forward(d, t->pending_carries, t->stream), "col_forward");
+        LNT_LAUNCH(lnt::launch_row_square(d, t->stream), "row_square");
+        LNT_LAUNCH(lnt::launch_col_inverse(d, t->canonical_input, t->stream), "col_inverse");
+      }
       t->pending_carries = true;
       t->canonical_input = false;
     }
@@ -427,6 +454,10 @@ int lnt_create(uint32_t exponent, uint32_t n, int prp, int device, lnt_test** ou
   } else {
     if ((st = upload_roots(t, plan.n1, &t->rt1, &t->irt1)) != LNT_OK) return bail(st);
     if ((st = upload_roots(t, plan.n2, &t->rt2, &t->irt2)) != LNT_OK) return bail(st);
+    if (plan.fast) {
+      if ((st = upload_roots(t, plan.n1, &t->itw1, &t->iitw1, true)) != LNT_OK) return bail(st);
+      if ((st = upload_roots(t, plan.n2, &t->itw2, &t->iitw2, true)) != LNT_OK) return bail(st);
+    }
     if ((e = dalloc(&t->twf, n)) || (e = dalloc(&t->twi, n)) ||
         (e = dalloc(&t->carry, (size_t)plan.ntiles * plan.n2)))
       return bail(cuda_fail(e, "allocate twiddles"));

@@ -92,16 +92,24 @@ bool make_plan(uint32_t n, Plan& plan) {
   }
   plan.kind = PlanKind::TwoPass;
   uint32_t l2 = plan.log2n / 2;
-  if (l2 > 11) l2 = 11;
   uint32_t l1 = plan.log2n - l2;
-  if (l1 > 14) { l1 = 14; l2 = plan.log2n - 14; }
+  if (fast_supported(l1, l2)) {
+    // register-radix kernels: columns of n2 = 64 * RB, rows of n1 = 64 * RB'
+    plan.fast = true;
+    plan.tile = fast_tile(l2);
+  } else {
+    if (l2 > 11) l2 = 11;
+    l1 = plan.log2n - l2;
+    if (l1 > 14) { l1 = 14; l2 = plan.log2n - 14; }
+    plan.tile = l2 <= 11 ? 8 : 4;
+  }
   plan.log2n1 = l1;
   plan.log2n2 = l2;
   plan.n1 = 1u << l1;
   plan.n2 = 1u << l2;
-  plan.tile = l2 <= 11 ? 8 : 4;
   plan.ntiles = plan.n1 / plan.tile;
-  plan.name = "TWOPASS_" + std::to_string(plan.n2) + "x" + std::to_string(plan.n1);
+  plan.name = "TWOPASS_" + std::to_string(plan.n2) + "x" + std::to_string(plan.n1) +
+              (plan.fast ? "_R64" : "_R2");
   return true;
 }
 

@@ -102,26 +102,20 @@ def make_c2(long_run: bool) -> None:
 
 
 def make_ref() -> None:
-    """Parse reference dumps: gpurun_out/ref_<tag>/<q>_<n>_<prp>_<iters>.dat"""
+    """Collect the reference runs summarised by oracle/run_ref.py on a B200
+    (gpurun_out/ref_*/run_*.json: Res64 of its LucasNTT_results.dat dump)."""
     base = ROOT / "gpurun_out"
     cases = []
-    for dat in sorted(base.glob("ref_*/*.dat")):
-        q, n, prp, iters = (int(x) for x in dat.stem.split("_"))
-        words = [int(line, 16) for line in dat.read_text().split()]
-        assert len(words) == n, dat
-        widths = B.widths(q, n)
-        r, pos = 0, 0
-        for d, w in zip(words, widths):
-            if pos >= 64:
-                break
-            r = (r + (d << pos)) & 0xFFFFFFFFFFFFFFFF
-            pos += w
-        cases.append({"q": q, "n": n, "prp": bool(prp), "iterations": iters,
-                      "res64": f"{r:016x}", "is_prime": all(x == 0 for x in words[1:]) and
-                      words[0] == (9 if prp else 0)})
+    for js in sorted(base.glob("ref_*/run_*.json")):
+        r = json.loads(js.read_text())
+        if r.get("rc") != 0 or not r.get("res64"):
+            continue
+        cases.append({"q": r["exponent"], "n": r["n"], "prp": r["prp"], "iterations": r["iterations"],
+                      "res64": r["res64"], "fft": r["fft_used"], "pool": r["pool"],
+                      "per_iteration_ms": r["per_iteration_ms"], "conclusion": r["conclusion"]})
     write("ref_residues.json", {
-        "source": "reference LucasNTT build (oracle/build_ref.sh) run on a B200; "
-                  "Res64 derived from its LucasNTT_results.dat dump",
+        "source": "reference LucasNTT build (oracle/build_ref.sh) run on a B200 by oracle/run_ref.py; "
+                  "Res64 derived from its residue dump",
         "cases": cases})
 
 

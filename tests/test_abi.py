@@ -71,3 +71,13 @@ def test_canonical_readout_host_build(tmp_path):
                     str(ROOT / "tests" / "native" / "canon_selftest.cpp")], check=True)
     r = subprocess.run([str(exe)], capture_output=True, text=True)
     assert r.returncode == 0 and r.stdout.startswith("ok"), r.stdout
+
+
+def test_register_ntt_host_build(tmp_path):
+    """ntt_core.cuh: register NTTs of 1..64 points against a naive DFT, and every
+    power-of-two shift against a 128-bit remainder."""
+    exe = tmp_path / "ntt_selftest"
+    subprocess.run(["g++", "-O1", "-std=c++17", "-ftemplate-depth=2000", "-o", str(exe),
+                    str(ROOT / "tests" / "native" / "ntt_selftest.cpp")], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0 and r.stdout.startswith("ok"), r.stdout

@@ -147,3 +147,24 @@ def test_two_pass_known_prime(lnt):
         assert T.plan.startswith("TWOPASS")
         T.iterate(132049 - 2)
         assert T.is_prime()
+
+
+def test_reference_build_residues(lnt):
+    """Res64 equal to the reference's own build (run on a B200): C1 full
+    tests at n = 2048 and 4096, and q = 139000003 after 1000 and 10000
+    squarings at n = 2^23."""
+    cases = json.loads((GOLDEN / "ref_residues.json").read_text())["cases"]
+    c2 = sorted((c for c in cases if c["q"] == 139000003), key=lambda c: c["iterations"])
+    for c in cases:
+        if c["q"] == 139000003:
+            continue
+        with lnt.LucasTest(c["q"], c["n"], c["prp"]) as T:
+            T.iterate(c["iterations"])
+            assert f"{T.res64():016x}" == c["res64"], c
+            assert T.is_prime() == (c["conclusion"] == "Prime")
+    with lnt.LucasTest(139000003, 1 << 23, False) as T:
+        done = 0
+        for c in c2:
+            T.iterate(c["iterations"] - done)
+            done = c["iterations"]
+            assert f"{T.res64():016x}" == c["res64"], c

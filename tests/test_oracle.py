@@ -113,3 +113,21 @@ def test_c1_fixture_consistency():
     for c in cases:
         assert c["is_prime"] == (c["q"] == 44497)
         assert (c["res64"] == "0" * 16) == (c["q"] == 44497)
+
+
+def test_oracle_fixtures_match_reference_build():
+    """The C1 and C2 oracle fixtures agree with residues the reference's own
+    build produced on a B200 (tests/golden/ref_residues.json)."""
+    ref = json.loads((GOLDEN / "ref_residues.json").read_text())["cases"]
+    c1 = {(c["q"], c["n"]): c["res64"] for c in json.loads((GOLDEN / "c1_oracle.json").read_text())["cases"]}
+    c2 = json.loads((GOLDEN / "c2_oracle.json").read_text())["res64_after"]
+    checked = 0
+    for c in ref:
+        if (c["q"], c["n"]) in c1 and c["iterations"] == c["q"] - 2:
+            assert c1[(c["q"], c["n"])] == c["res64"], c
+            checked += 1
+        elif c["q"] == 139000003 and str(c["iterations"]) in c2:
+            assert c2[str(c["iterations"])] == c["res64"], c
+            checked += 1
+    assert checked >= 11
+    assert {c["conclusion"] for c in ref if c["q"] == 44497} == {"Prime"}
