@@ -29,9 +29,10 @@ GL_HD uint64_t mulhi(uint64_t a, uint64_t b) {
 }
 
 GL_HD uint64_t add(uint64_t a, uint64_t b) {
-  uint64_t s = a + b;
-  // s < a: the sum wrapped past 2^64, and s - p == s + EPS is the answer.
-  return (s < a || s >= P) ? s - P : s;
+  // a + b - p = a - (p - b): one subtraction and one conditional correction
+  const uint64_t t = P - b;
+  const uint64_t d = a - t;
+  return (a < t) ? d + P : d;
 }
 
 GL_HD uint64_t sub(uint64_t a, uint64_t b) {

@@ -39,6 +39,8 @@ struct lnt_test {
   uint64_t *twf = nullptr, *twi = nullptr;
   uint64_t *rt1 = nullptr, *irt1 = nullptr, *rt2 = nullptr, *irt2 = nullptr;
   uint64_t *itw1 = nullptr, *iitw1 = nullptr, *itw2 = nullptr, *iitw2 = nullptr;
+  uint64_t *wt = nullptr, *uwt = nullptr;
+  uint8_t* widt = nullptr;
   int64_t* carry = nullptr;
   // canonical readout
   uint64_t* canon = nullptr;
@@ -96,7 +98,7 @@ cudaError_t dalloc(T** p, size_t count) {
 void free_all(lnt_test* t) {
   void* ptrs[] = {t->x, t->w, t->uw, t->widths, t->status, t->rt, t->irt, t->rdesc,
                   t->twf, t->twi, t->rt1, t->irt1, t->rt2, t->irt2, t->itw1, t->iitw1,
-                  t->itw2, t->iitw2, t->carry, t->canon,
+                  t->itw2, t->iitw2, t->wt, t->uwt, t->widt, t->carry, t->canon,
                   t->blk_carry, t->blk_fn, t->blk_cin, t->cflags};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -114,7 +116,7 @@ void root_table(uint32_t n, bool inverse, std::vector<uint64_t>& out) {
   for (size_t k = 1; k < half; ++k) out[k] = gl::mul(out[k - 1], r);
 }
 
-// omega_n^e for all e < n (the fast kernels index it with i1 * k2 < n).
+// omega_n^e for all e < n (the radix-16 kernels index it with t * k * span_scale < n).
 void power_table(uint32_t n, bool inverse, std::vector<uint64_t>& out) {
   uint64_t r = gl::pow(554, (gl::P - 1) / n);
   if (inverse) r = gl::inv(r);
@@ -157,6 +159,9 @@ lnt::TwoPassDesc twopass_desc(const lnt_test* t) {
   d.iitw1 = t->iitw1;
   d.itw2 = t->itw2;
   d.iitw2 = t->iitw2;
+  d.wt = t->wt;
+  d.uwt = t->uwt;
+  d.widt = t->widt;
   d.status = t->status;
   d.n1 = t->plan.n1;
   d.n2 = t->plan.n2;
@@ -351,9 +356,9 @@ int queue_iterations(lnt_test* t, uint64_t iterations, LaunchTimer* timer) {
     lnt::TwoPassDesc d = twopass_desc(t);
     for (uint64_t i = 0; i < iterations; ++i) {
       if (t->plan.fast) {
-        LNT_LAUNCH(lnt::launch_col_forward_fast(d, t->pending_carries, t->stream), "col_forward");
-        LNT_LAUNCH(lnt::launch_row_square_fast(d, t->stream), "row_square");
-        LNT_LAUNCH(lnt::launch_col_inverse_fast(d, t->canonical_input, t->stream), "col_inverse");
+        LNT_LAUNCH(lnt::launch_col_forward_r16(d, t->pending_carries, t->stream), "col_forward");
+        LNT_LAUNCH(lnt::launch_row_square_r16(d, t->stream), "row_square");
+        LNT_LAUNCH(lnt::launch_col_inverse_r16(d, t->canonical_input, t->stream), "col_inverse");
       } else {
         LNT_LAUNCH(lnt::launch_col_forward(d, t->pending_carries, t->stream), "col_forward");
         LNT_LAUNCH(lnt::launch_row_square(d, t->stream), "row_square");
@@ -457,6 +462,10 @@ int lnt_create(uint32_t exponent, uint32_t n, int prp, int device, lnt_test** ou
     if (plan.fast) {
       if ((st = upload_roots(t, plan.n1, &t->itw1, &t->iitw1, true)) != LNT_OK) return bail(st);
       if ((st = upload_roots(t, plan.n2, &t->itw2, &t->iitw2, true)) != LNT_OK) return bail(st);
+      if ((e = dalloc(&t->wt, n)) || (e = dalloc(&t->uwt, n)) || (e = dalloc(&t->widt, n)) ||
+          (e = lnt::launch_tile_major(t->w, t->uw, t->widths, plan.n1, plan.n2, plan.tile, t->wt,
+                                      t->uwt, t->widt, t->stream)))
+        return bail(cuda_fail(e, "tile-major tables"));
     }
     if ((e = dalloc(&t->twf, n)) || (e = dalloc(&t->twi, n)) ||
         (e = dalloc(&t->carry, (size_t)plan.ntiles * plan.n2)))

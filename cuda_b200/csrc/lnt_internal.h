@@ -27,7 +27,7 @@ struct Plan {
   uint32_t n1 = 0, n2 = 0, log2n1 = 0, log2n2 = 0;
   uint32_t tile = 0;    // columns per column-pass CTA = words per carry run
   uint32_t ntiles = 0;  // n1 / tile
-  bool fast = false;    // register-radix kernels (lnt_fastpass.cu) instead of radix-2
+  bool fast = false;    // radix-16 pass kernels (lnt_radix16.cu) instead of radix-2
   std::string name;
 };
 
@@ -71,10 +71,15 @@ struct TwoPassDesc {
   const uint64_t* irt1;
   const uint64_t* rt2;    // column roots omega_n2^k, k < n2/2
   const uint64_t* irt2;
-  const uint64_t* itw1;   // fast kernels: omega_n1^e, e < n1 (and inverses)
+  const uint64_t* itw1;   // radix-16 kernels: omega_n1^e, e < n1 (and inverses)
   const uint64_t* iitw1;
-  const uint64_t* itw2;   // fast kernels: omega_n2^e, e < n2 (and inverses)
+  const uint64_t* itw2;   // radix-16 kernels: omega_n2^e, e < n2 (and inverses)
   const uint64_t* iitw2;
+  // radix-16 column kernels: w, uw, widths in tile-major order, index
+  // (tile * n2 + row) * tile_width + column-in-tile, so a row's run is contiguous
+  const uint64_t* wt;
+  const uint64_t* uwt;
+  const uint8_t* widt;
   uint32_t* status;
   uint32_t n1, n2, log2n1, log2n2, tile, ntiles;
   uint32_t prp;
@@ -84,18 +89,21 @@ cudaError_t launch_col_forward(const TwoPassDesc& d, bool apply_carries, cudaStr
 cudaError_t launch_row_square(const TwoPassDesc& d, cudaStream_t s);
 cudaError_t launch_col_inverse(const TwoPassDesc& d, bool unsigned_mode, cudaStream_t s);
 
-// register-radix variants (lnt_fastpass.cu): n2, n1 in [2^8, 2^12], n1 >= n2
-bool fast_supported(uint32_t log2n1, uint32_t log2n2);
-uint32_t fast_tile(uint32_t log2n2);
-cudaError_t launch_col_forward_fast(const TwoPassDesc& d, bool apply_carries, cudaStream_t s);
-cudaError_t launch_row_square_fast(const TwoPassDesc& d, cudaStream_t s);
-cudaError_t launch_col_inverse_fast(const TwoPassDesc& d, bool unsigned_mode, cudaStream_t s);
+// radix-16 pass variants (lnt_radix16.cu): n2 in [2^6, 2^12], n1 in [2^7, 2^12], n1 >= n2
+bool r16_supported(uint32_t log2n1, uint32_t log2n2);
+uint32_t r16_tile(uint32_t log2n2);
+cudaError_t launch_col_forward_r16(const TwoPassDesc& d, bool apply_carries, cudaStream_t s);
+cudaError_t launch_row_square_r16(const TwoPassDesc& d, cudaStream_t s);
+cudaError_t launch_col_inverse_r16(const TwoPassDesc& d, bool unsigned_mode, cudaStream_t s);
 
 // ------------------------------------------------------------- tables ----
 cudaError_t launch_weights(uint32_t exponent, uint32_t n, uint64_t* w, uint64_t* uw,
                            cudaStream_t s);
 cudaError_t launch_twiddles(uint32_t n1, uint32_t n2, uint32_t log2n2, uint64_t* twf,
                             uint64_t* twi, cudaStream_t s);
+cudaError_t launch_tile_major(const uint64_t* w, const uint64_t* uw, const uint8_t* widths,
+                              uint32_t n1, uint32_t n2, uint32_t tile, uint64_t* wt, uint64_t* uwt,
+                              uint8_t* widt, cudaStream_t s);
 
 // --------------------------------------------------- canonical readout ----
 struct CanonDesc {

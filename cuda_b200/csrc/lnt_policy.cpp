@@ -93,10 +93,10 @@ bool make_plan(uint32_t n, Plan& plan) {
   plan.kind = PlanKind::TwoPass;
   uint32_t l2 = plan.log2n / 2;
   uint32_t l1 = plan.log2n - l2;
-  if (fast_supported(l1, l2)) {
-    // register-radix kernels: columns of n2 = 64 * RB, rows of n1 = 64 * RB'
+  if (r16_supported(l1, l2)) {
+    // radix-16 pass kernels
     plan.fast = true;
-    plan.tile = fast_tile(l2);
+    plan.tile = r16_tile(l2);
   } else {
     if (l2 > 11) l2 = 11;
     l1 = plan.log2n - l2;
@@ -109,7 +109,7 @@ bool make_plan(uint32_t n, Plan& plan) {
   plan.n2 = 1u << l2;
   plan.ntiles = plan.n1 / plan.tile;
   plan.name = "TWOPASS_" + std::to_string(plan.n2) + "x" + std::to_string(plan.n1) +
-              (plan.fast ? "_R64" : "_R2");
+              (plan.fast ? "_R16" : "_R2");
   return true;
 }
 

@@ -1,0 +1,392 @@
+// Two-pass squaring with radix-16 register passes (n = 2^13 ... 2^24).
+//
+// Same layout, twiddle tables and carry scheme as lnt_twopass.cu (which
+// replaces the reference's FFT_2SMEM pool, kernel_pool.cu:39-48).  A transform
+// of length L = r0 * r1 * ... (every r <= 16, a power of two) runs as passes
+// over shared memory: pass j takes R = r_j elements at stride span_j / R from a
+// block of span_j = L / (r0 ... r_{j-1}) words into registers, does an R-point
+// DIF with power-of-two twiddles (ntt_core.cuh), multiplies by
+// omega_span^(t * k) and writes back.  The result is in fully bit-reversed order,
+// like the radix-2 kernels, so all plans share the 4-step twiddle tables.
+// Per element a pass costs log2(R) shift butterflies and one table
+// multiplication; the reference pays one general modular multiplication per
+// radix-2 butterfly (core/fft_r2.cuh:17-107).
+//
+// Small unrolled bodies (one 16-point transform) inside runtime loops keep the
+// kernels small enough for the instruction cache; fully unrolled 64-point
+// passes starved the SM of instructions.  Shared memory is padded by one word
+// in 16 (sw below), which makes every pass stride bank-conflict free.
+//
+// row_square_r16: the first pass reads HBM directly (with the 4-step twiddle)
+// and the last inverse pass writes HBM directly; the last forward pass, the
+// pointwise square and the first inverse pass run in registers back to back.
+#include "carry.cuh"
+#include "lnt_internal.h"
+#include "ntt_core.cuh"
+
+namespace lnt {
+
+namespace {
+
+__device__ __forceinline__ int sw(int i) { return i + (i >> 4); }
+__host__ __device__ constexpr int padded(int L) { return L + L / 16; }
+
+struct Passes {
+  int m;          // number of passes
+  int radix[4];   // r_0 (largest stride) ... r_{m-1} (contiguous)
+};
+
+Passes make_passes(int log2L) {
+  Passes p{};
+  int first = log2L % 4;
+  int rest = log2L - first;
+  if (first == 0) {
+    first = 4;
+    rest -= 4;
+  }
+  p.radix[p.m++] = 1 << first;
+  for (int k = 0; k < rest / 4; ++k) p.radix[p.m++] = 16;
+  return p;
+}
+
+// ---- one task: R elements of one block, forward or inverse ----------------
+
+// forward: DIF, then omega_span^(t k) (table of omega_L, scaled by L / span)
+template <int R>
+__device__ __forceinline__ void task_dif(uint64_t* base, int off, int q, int t, const uint64_t* twL,
+                                         int tws) {
+  uint64_t v[R];
+#pragma unroll
+  for (int d = 0; d < R; ++d) v[d] = base[sw(off + q * d)];
+  dif<R>(v);
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    uint64_t x = v[r];
+    if (q > 1) x = gl::mul(x, twL[t * brev_c<R>(r) * tws]);
+    base[sw(off + q * r)] = x;
+  }
+}
+
+// inverse: omega_span^-(t k), then DIT
+template <int R>
+__device__ __forceinline__ void task_dit(uint64_t* base, int off, int q, int t, const uint64_t* itwL,
+                                         int tws) {
+  uint64_t v[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    uint64_t x = base[sw(off + q * r)];
+    if (q > 1) x = gl::mul(x, itwL[t * brev_c<R>(r) * tws]);
+    v[r] = x;
+  }
+  dit_inv<R>(v);
+#pragma unroll
+  for (int d = 0; d < R; ++d) base[sw(off + q * d)] = v[d];
+}
+
+// last forward pass, pointwise square and first inverse pass (contiguous blocks)
+template <int R>
+__device__ __forceinline__ void task_square(uint64_t* base, int off) {
+  uint64_t v[R];
+#pragma unroll
+  for (int d = 0; d < R; ++d) v[d] = base[sw(off + d)];
+  dif<R>(v);
+#pragma unroll
+  for (int d = 0; d < R; ++d) v[d] = gl::sqr(v[d]);
+  dit_inv<R>(v);
+#pragma unroll
+  for (int d = 0; d < R; ++d) base[sw(off + d)] = v[d];
+}
+
+// A pass over `ntrans` transforms of length L; transform g lives at sm + g * ld.
+template <int R, int Mode>  // Mode 0: DIF, 1: DIT, 2: square
+__device__ void pass(uint64_t* sm, int ld, int ntrans, int L, int span, const uint64_t* tw) {
+  const int q = span / R, per = L / R, tws = L / span;
+  const int total = ntrans * per;
+  for (int task = threadIdx.x; task < total; task += blockDim.x) {
+    const int g = task / per, k = task % per;
+    const int b = k / q, t = k % q;
+    uint64_t* base = sm + g * ld;
+    if constexpr (Mode == 0)
+      task_dif<R>(base, b * span + t, q, t, tw, tws);
+    else if constexpr (Mode == 1)
+      task_dit<R>(base, b * span + t, q, t, tw, tws);
+    else
+      task_square<R>(base, b * span);
+  }
+}
+
+template <int Mode>
+__device__ __forceinline__ void pass_r(int R, uint64_t* sm, int ld, int ntrans, int L, int span,
+                                       const uint64_t* tw) {
+  switch (R) {
+    case 2: pass<2, Mode>(sm, ld, ntrans, L, span, tw); break;
+    case 4: pass<4, Mode>(sm, ld, ntrans, L, span, tw); break;
+    case 8: pass<8, Mode>(sm, ld, ntrans, L, span, tw); break;
+    default: pass<16, Mode>(sm, ld, ntrans, L, span, tw); break;
+  }
+}
+
+// ------------------------------------------------------------------ rows ----
+
+constexpr int kRowThreads = 256;
+
+// first pass fused with the HBM read and the 4-step twiddle
+template <int R>
+__device__ void row_first_pass(uint64_t* sm, int ld, int rows, int L, const uint64_t* x,
+                               const uint64_t* twf, const uint64_t* twL) {
+  const int q = L / R;
+  for (int task = threadIdx.x; task < rows * q; task += blockDim.x) {
+    const int g = task / q, t = task % q;
+    const size_t rb = (size_t)g * L;
+    uint64_t v[R];
+#pragma unroll
+    for (int d = 0; d < R; ++d) v[d] = gl::mul(x[rb + t + q * d], twf[rb + t + q * d]);
+    dif<R>(v);
+#pragma unroll
+    for (int r = 0; r < R; ++r) sm[g * ld + sw(t + q * r)] = gl::mul(v[r], twL[t * brev_c<R>(r)]);
+  }
+}
+
+// last inverse pass fused with the inverse 4-step twiddle and the HBM write
+template <int R>
+__device__ void row_last_pass(const uint64_t* sm, int ld, int rows, int L, uint64_t* x,
+                              const uint64_t* twi, const uint64_t* itwL) {
+  const int q = L / R;
+  for (int task = threadIdx.x; task < rows * q; task += blockDim.x) {
+    const int g = task / q, t = task % q;
+    const size_t rb = (size_t)g * L;
+    uint64_t v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = gl::mul(sm[g * ld + sw(t + q * r)], itwL[t * brev_c<R>(r)]);
+    dit_inv<R>(v);
+#pragma unroll
+    for (int d = 0; d < R; ++d) x[rb + t + q * d] = gl::mul(v[d], twi[rb + t + q * d]);
+  }
+}
+
+__global__ void __launch_bounds__(kRowThreads) row_square_r16(TwoPassDesc D, Passes P, int rows) {
+  extern __shared__ __align__(16) uint64_t sm[];
+  const int L = (int)D.n1, ld = padded(L);
+  const size_t off = (size_t)blockIdx.x * rows * L;
+  uint64_t* x = reinterpret_cast<uint64_t*>(D.x) + off;
+  switch (P.radix[0]) {
+    case 2: row_first_pass<2>(sm, ld, rows, L, x, D.twf + off, D.itw1); break;
+    case 4: row_first_pass<4>(sm, ld, rows, L, x, D.twf + off, D.itw1); break;
+    case 8: row_first_pass<8>(sm, ld, rows, L, x, D.twf + off, D.itw1); break;
+    default: row_first_pass<16>(sm, ld, rows, L, x, D.twf + off, D.itw1); break;
+  }
+  __syncthreads();
+  int span = L / P.radix[0];
+  for (int j = 1; j + 1 < P.m; ++j) {
+    pass_r<0>(P.radix[j], sm, ld, rows, L, span, D.itw1);
+    span /= P.radix[j];
+    __syncthreads();
+  }
+  pass_r<2>(P.radix[P.m - 1], sm, ld, rows, L, span, nullptr);
+  __syncthreads();
+  for (int j = P.m - 2; j >= 1; --j) {
+    span *= P.radix[j];
+    pass_r<1>(P.radix[j], sm, ld, rows, L, span, D.iitw1);
+    __syncthreads();
+  }
+  switch (P.radix[0]) {
+    case 2: row_last_pass<2>(sm, ld, rows, L, x, D.twi + off, D.iitw1); break;
+    case 4: row_last_pass<4>(sm, ld, rows, L, x, D.twi + off, D.iitw1); break;
+    case 8: row_last_pass<8>(sm, ld, rows, L, x, D.twi + off, D.iitw1); break;
+    default: row_last_pass<16>(sm, ld, rows, L, x, D.twi + off, D.iitw1); break;
+  }
+}
+
+// --------------------------------------------------------------- columns ----
+
+constexpr int kColThreads = 512;
+
+// column stride in words: the coalesced staging (lanes = T columns x 32/T
+// rows) then hits distinct banks
+__host__ __device__ constexpr int col_ld(int L, int T) {
+  return ((padded(L) + 15) / 16) * 16 + (T >= 16 ? 1 : 16 / T);
+}
+
+__device__ __forceinline__ void tile_load(uint64_t* sm, int ld, const int64_t* x, int L, int T,
+                                          uint32_t n1, uint32_t c0) {
+  for (int idx = threadIdx.x; idx < T * L; idx += blockDim.x) {
+    const int r = idx / T, c = idx % T;
+    sm[c * ld + sw(r)] = (uint64_t)x[(size_t)r * n1 + c0 + c];
+  }
+}
+
+__device__ __forceinline__ void tile_store(const uint64_t* sm, int ld, int64_t* x, int L, int T,
+                                           uint32_t n1, uint32_t c0) {
+  for (int idx = threadIdx.x; idx < T * L; idx += blockDim.x) {
+    const int r = idx / T, c = idx % T;
+    x[(size_t)r * n1 + c0 + c] = (int64_t)sm[c * ld + sw(r)];
+  }
+}
+
+// A row's run of T table entries, read as 16-byte vectors (tile-major tables:
+// the run is contiguous and consecutive rows are adjacent, so a warp's loads
+// are coalesced).
+template <int T>
+__device__ __forceinline__ void load_run(const uint64_t* src, uint64_t (&out)[T]) {
+  const ulonglong2* v = reinterpret_cast<const ulonglong2*>(src);
+#pragma unroll
+  for (int k = 0; k < T / 2; ++k) {
+    const ulonglong2 u = v[k];
+    out[2 * k] = u.x;
+    out[2 * k + 1] = u.y;
+  }
+}
+
+template <int T>
+__device__ __forceinline__ void load_widths(const uint8_t* src, unsigned (&out)[T]) {
+  if constexpr (T == 8) {
+    const uint64_t u = *reinterpret_cast<const uint64_t*>(src);
+#pragma unroll
+    for (int c = 0; c < 8; ++c) out[c] = (unsigned)((u >> (8 * c)) & 0xFF);
+  } else {
+    const uint32_t u = *reinterpret_cast<const uint32_t*>(src);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) out[c] = (u >> (8 * c)) & 0xFF;
+  }
+}
+
+template <int T>
+__global__ void __launch_bounds__(kColThreads) col_forward_r16(TwoPassDesc D, Passes P,
+                                                               int apply_carries) {
+  extern __shared__ __align__(16) uint64_t sm[];
+  const int L = (int)D.n2, ld = col_ld(L, T);
+  const uint32_t n1 = D.n1, t0 = blockIdx.x, c0 = t0 * T;
+  uint32_t status = 0;
+
+  tile_load(sm, ld, D.x, L, T, n1, c0);
+  __syncthreads();
+  // per row: carry from the previous run, then weight (balanced digit -> field)
+  for (int r = threadIdx.x; r < L; r += blockDim.x) {
+    const size_t run = (size_t)t0 * L + r;
+    uint64_t w[T];
+    unsigned wd[T];
+    load_run<T>(D.wt + run * T, w);
+    load_widths<T>(D.widt + run * T, wd);
+    int64_t carry = 0;
+    if (apply_carries) carry = D.carry[t0 > 0 ? run - L : (size_t)(D.ntiles - 1) * L + (r ? r - 1 : L - 1)];
+#pragma unroll
+    for (int c = 0; c < T; ++c) {
+      uint64_t& v = sm[c * ld + sw(r)];
+      int64_t d = (int64_t)v;
+      if (carry != 0) {
+        if (c + 1 < T) {
+          int64_t q;
+          d = balance(d + carry, wd[c], q);
+          carry = q;
+        } else {
+          d += carry;
+          if (carry > kAbsorbLimit || carry < -kAbsorbLimit) status |= kStatusCarryOverflow;
+          carry = 0;
+        }
+      }
+      v = gl::mul(gl::from_signed(d), w[c]);
+    }
+  }
+  __syncthreads();
+  int span = L;
+  for (int j = 0; j < P.m; ++j) {
+    pass_r<0>(P.radix[j], sm, ld, T, L, span, D.itw2);
+    span /= P.radix[j];
+    __syncthreads();
+  }
+  tile_store(sm, ld, D.x, L, T, n1, c0);
+  if (status) atomicOr(D.status, status);
+}
+
+template <int T>
+__global__ void __launch_bounds__(kColThreads) col_inverse_r16(TwoPassDesc D, Passes P,
+                                                               int unsigned_mode) {
+  extern __shared__ __align__(16) uint64_t sm[];
+  const int L = (int)D.n2, ld = col_ld(L, T);
+  const uint32_t n1 = D.n1, t0 = blockIdx.x, c0 = t0 * T;
+
+  tile_load(sm, ld, D.x, L, T, n1, c0);
+  __syncthreads();
+  int span = 1;
+  for (int j = P.m - 1; j >= 0; --j) {
+    span *= P.radix[j];
+    pass_r<1>(P.radix[j], sm, ld, T, L, span, D.iitw2);
+    __syncthreads();
+  }
+  // per row: unweight, carry the run of T words to balanced digits, minus two
+  for (int r = threadIdx.x; r < L; r += blockDim.x) {
+    const size_t run = (size_t)t0 * L + r;
+    uint64_t uw[T];
+    unsigned wd[T];
+    load_run<T>(D.uwt + run * T, uw);
+    load_widths<T>(D.widt + run * T, wd);
+    int64_t carry = (!D.prp && t0 == 0 && r == 0) ? -2 : 0;
+#pragma unroll
+    for (int c = 0; c < T; ++c) {
+      uint64_t& v = sm[c * ld + sw(r)];
+      int64_t hi, lo, q;
+      split_output(gl::mul(v, uw[c]), unsigned_mode != 0, wd[c], hi, lo);
+      v = (uint64_t)balance(lo + carry, wd[c], q);
+      carry = hi + q;
+    }
+    D.carry[run] = carry;
+  }
+  __syncthreads();
+  tile_store(sm, ld, D.x, L, T, n1, c0);
+}
+
+int row_rows_per_cta(int L, int n2) {
+  int rows = 8192 / L;
+  if (rows < 1) rows = 1;
+  while (rows > 1 && n2 / rows < 148) rows /= 2;
+  return rows;
+}
+
+}  // namespace
+
+bool r16_supported(uint32_t log2n1, uint32_t log2n2) {
+  return log2n2 >= 6 && log2n2 <= 12 && log2n1 >= 7 && log2n1 <= 12 && log2n1 >= log2n2;
+}
+
+uint32_t r16_tile(uint32_t log2n2) { return log2n2 >= 12 ? 4 : 8; }
+
+cudaError_t launch_row_square_r16(const TwoPassDesc& d, cudaStream_t s) {
+  const int L = (int)d.n1, rows = row_rows_per_cta(L, (int)d.n2);
+  const size_t smem = (size_t)rows * padded(L) * 8;
+  cudaError_t e = cudaFuncSetAttribute(row_square_r16, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  row_square_r16<<<d.n2 / rows, kRowThreads, smem, s>>>(d, make_passes((int)d.log2n1), rows);
+  return cudaGetLastError();
+}
+
+template <int T>
+cudaError_t col_forward_t(const TwoPassDesc& d, bool apply, cudaStream_t s) {
+  const size_t smem = (size_t)T * col_ld((int)d.n2, T) * 8;
+  cudaError_t e = cudaFuncSetAttribute(col_forward_r16<T>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  col_forward_r16<T><<<d.ntiles, kColThreads, smem, s>>>(d, make_passes((int)d.log2n2), apply ? 1 : 0);
+  return cudaGetLastError();
+}
+
+template <int T>
+cudaError_t col_inverse_t(const TwoPassDesc& d, bool unsigned_mode, cudaStream_t s) {
+  const size_t smem = (size_t)T * col_ld((int)d.n2, T) * 8;
+  cudaError_t e = cudaFuncSetAttribute(col_inverse_r16<T>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  col_inverse_r16<T><<<d.ntiles, kColThreads, smem, s>>>(d, make_passes((int)d.log2n2),
+                                                         unsigned_mode ? 1 : 0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_col_forward_r16(const TwoPassDesc& d, bool apply, cudaStream_t s) {
+  return d.tile == 4 ? col_forward_t<4>(d, apply, s) : col_forward_t<8>(d, apply, s);
+}
+
+cudaError_t launch_col_inverse_r16(const TwoPassDesc& d, bool unsigned_mode, cudaStream_t s) {
+  return d.tile == 4 ? col_inverse_t<4>(d, unsigned_mode, s) : col_inverse_t<8>(d, unsigned_mode, s);
+}
+
+}  // namespace lnt

@@ -40,7 +40,30 @@ __global__ void twiddle_kernel(uint32_t n1, uint32_t n2, uint32_t log2n2, uint64
   twi[idx] = gl::pow(iroot, e);
 }
 
+// natural index j = r * n1 + t * tile + c  ->  (t * n2 + r) * tile + c
+__global__ void tile_major_kernel(const uint64_t* w, const uint64_t* uw, const uint8_t* widths,
+                                  uint32_t n1, uint32_t n2, uint32_t tile, uint64_t* wt,
+                                  uint64_t* uwt, uint8_t* widt) {
+  const size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= (size_t)n1 * n2) return;
+  const uint32_t r = (uint32_t)(j / n1), col = (uint32_t)(j % n1);
+  const uint32_t t = col / tile, c = col % tile;
+  const size_t k = ((size_t)t * n2 + r) * tile + c;
+  wt[k] = w[j];
+  uwt[k] = uw[j];
+  widt[k] = widths[j];
+}
+
 }  // namespace
+
+cudaError_t launch_tile_major(const uint64_t* w, const uint64_t* uw, const uint8_t* widths,
+                              uint32_t n1, uint32_t n2, uint32_t tile, uint64_t* wt, uint64_t* uwt,
+                              uint8_t* widt, cudaStream_t s) {
+  const uint64_t n = (uint64_t)n1 * n2;
+  tile_major_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(w, uw, widths, n1, n2, tile, wt, uwt,
+                                                                 widt);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_weights(uint32_t exponent, uint32_t n, uint64_t* w, uint64_t* uw,
                            cudaStream_t s) {

@@ -27,6 +27,13 @@ GL_HD uint64_t shl_c(uint64_t x) {
     return x;
   } else if constexpr (S >= 96) {
     return gl::neg(shl_c<S - 96>(x));  // 2^96 = -1
+  } else if constexpr (S <= 32) {
+    // x 2^S = lo + 2^64 hi with hi < 2^32: lo + hi (2^32 - 1)
+    const uint64_t lo = x << S, hi = x >> (64 - S);
+    const uint64_t m = (hi << 32) - hi;
+    uint64_t r = lo + m;
+    if (r < m) r += gl::EPS;
+    return r >= gl::P ? r - gl::P : r;
   } else if constexpr (S < 64) {
     return gl::reduce128(x << S, x >> (64 - S));
   } else {
