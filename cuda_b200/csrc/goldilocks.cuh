@@ -28,16 +28,53 @@ GL_HD uint64_t mulhi(uint64_t a, uint64_t b) {
 #endif
 }
 
+#if defined(__CUDA_ARCH__)
+// a - b with the 32-bit carry chain: the borrow of the subtraction itself
+// selects the correction (+p: low word + 1, high word + 2^32 - 1), no compare.
+__device__ __forceinline__ uint64_t sub_chain(uint32_t a0, uint32_t a1, uint32_t b0, uint32_t b1) {
+  uint32_t d0, d1, m;
+  asm("{\n\t"
+      "sub.cc.u32  %0, %3, %5;\n\t"
+      "subc.cc.u32 %1, %4, %6;\n\t"
+      "subc.u32    %2, 0, 0;\n\t"
+      "}"
+      : "=r"(d0), "=r"(d1), "=r"(m)
+      : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
+  asm("{\n\t"
+      "add.cc.u32 %0, %0, %2;\n\t"
+      "addc.u32   %1, %1, %3;\n\t"
+      "}"
+      : "+r"(d0), "+r"(d1)
+      : "r"(m & 1u), "r"(m));
+  return ((uint64_t)d1 << 32) | d0;
+}
+#endif
+
+GL_HD uint64_t sub(uint64_t a, uint64_t b) {
+#if defined(__CUDA_ARCH__)
+  return sub_chain((uint32_t)a, (uint32_t)(a >> 32), (uint32_t)b, (uint32_t)(b >> 32));
+#else
+  uint64_t d = a - b;
+  return (a < b) ? d + P : d;
+#endif
+}
+
 GL_HD uint64_t add(uint64_t a, uint64_t b) {
   // a + b - p = a - (p - b): one subtraction and one conditional correction
+#if defined(__CUDA_ARCH__)
+  uint32_t t0, t1;
+  asm("{\n\t"
+      "sub.cc.u32 %0, 1, %2;\n\t"
+      "subc.u32   %1, 0xFFFFFFFF, %3;\n\t"
+      "}"
+      : "=r"(t0), "=r"(t1)
+      : "r"((uint32_t)b), "r"((uint32_t)(b >> 32)));
+  return sub_chain((uint32_t)a, (uint32_t)(a >> 32), t0, t1);
+#else
   const uint64_t t = P - b;
   const uint64_t d = a - t;
   return (a < t) ? d + P : d;
-}
-
-GL_HD uint64_t sub(uint64_t a, uint64_t b) {
-  uint64_t d = a - b;
-  return (a < b) ? d + P : d;
+#endif
 }
 
 GL_HD uint64_t neg(uint64_t a) { return a ? P - a : 0; }

@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(kRowThreads) row_square_r16(TwoPassDesc D, Pas
 
 // --------------------------------------------------------------- columns ----
 
-constexpr int kColThreads = 512;
+constexpr int kColThreads = 1024;
 
 // column stride in words: the coalesced staging (lanes = T columns x 32/T
 // rows) then hits distinct banks
@@ -207,19 +207,38 @@ __host__ __device__ constexpr int col_ld(int L, int T) {
   return ((padded(L) + 15) / 16) * 16 + (T >= 16 ? 1 : 16 / T);
 }
 
+// HBM -> shared memory without a register round trip: every word is an
+// 8-byte cp.async, so all of a thread's loads are in flight together.
 __device__ __forceinline__ void tile_load(uint64_t* sm, int ld, const int64_t* x, int L, int T,
                                           uint32_t n1, uint32_t c0) {
   for (int idx = threadIdx.x; idx < T * L; idx += blockDim.x) {
     const int r = idx / T, c = idx % T;
-    sm[c * ld + sw(r)] = (uint64_t)x[(size_t)r * n1 + c0 + c];
+    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(sm + c * ld + sw(r));
+    const int64_t* src = x + (size_t)r * n1 + c0 + c;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src) : "memory");
   }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
+// shared memory -> HBM, four words per thread per round so the shared-memory
+// reads overlap
 __device__ __forceinline__ void tile_store(const uint64_t* sm, int ld, int64_t* x, int L, int T,
                                            uint32_t n1, uint32_t c0) {
-  for (int idx = threadIdx.x; idx < T * L; idx += blockDim.x) {
-    const int r = idx / T, c = idx % T;
-    x[(size_t)r * n1 + c0 + c] = (int64_t)sm[c * ld + sw(r)];
+  const int total = T * L, step = blockDim.x;
+  if (total % (4 * step) != 0) {
+    for (int idx = threadIdx.x; idx < total; idx += step)
+      x[(size_t)(idx / T) * n1 + c0 + idx % T] = (int64_t)sm[(idx % T) * ld + sw(idx / T)];
+    return;
+  }
+  for (int base = threadIdx.x; base < total; base += 4 * step) {
+    const uint64_t v0 = sm[(base % T) * ld + sw(base / T)];
+    const uint64_t v1 = sm[((base + step) % T) * ld + sw((base + step) / T)];
+    const uint64_t v2 = sm[((base + 2 * step) % T) * ld + sw((base + 2 * step) / T)];
+    const uint64_t v3 = sm[((base + 3 * step) % T) * ld + sw((base + 3 * step) / T)];
+    x[(size_t)(base / T) * n1 + c0 + base % T] = (int64_t)v0;
+    x[(size_t)((base + step) / T) * n1 + c0 + (base + step) % T] = (int64_t)v1;
+    x[(size_t)((base + 2 * step) / T) * n1 + c0 + (base + 2 * step) % T] = (int64_t)v2;
+    x[(size_t)((base + 3 * step) / T) * n1 + c0 + (base + 3 * step) % T] = (int64_t)v3;
   }
 }
 
