@@ -90,7 +90,43 @@ GL_HD uint64_t reduce128(uint64_t lo, uint64_t hi) {
   return r >= P ? r - P : r;
 }
 
-GL_HD uint64_t mul(uint64_t a, uint64_t b) { return reduce128(a * b, mulhi(a, b)); }
+GL_HD uint64_t mul(uint64_t a, uint64_t b) {
+#if defined(__CUDA_ARCH__)
+  // 128-bit product from 32-bit limbs (multiplier pipe), then the reduction
+  // lo + r2 (2^32 - 1) - r3 with carry chains.
+  uint32_t r0, r1, r2, r3;
+  asm("{\n\t"
+      "mul.lo.u32     %0, %4, %6;\n\t"
+      "mul.hi.u32     %1, %4, %6;\n\t"
+      "mad.lo.cc.u32  %1, %4, %7, %1;\n\t"
+      "madc.hi.u32    %2, %4, %7, 0;\n\t"
+      "mad.lo.cc.u32  %1, %5, %6, %1;\n\t"
+      "madc.hi.cc.u32 %2, %5, %6, %2;\n\t"
+      "madc.hi.u32    %3, %5, %7, 0;\n\t"
+      "mad.lo.cc.u32  %2, %5, %7, %2;\n\t"
+      "addc.u32       %3, %3, 0;\n\t"
+      "}"
+      : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+      : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)), "r"((uint32_t)b), "r"((uint32_t)(b >> 32)));
+  uint32_t t0, t1, m;
+  asm("{\n\tsub.cc.u32 %0, %3, %5;\n\tsubc.cc.u32 %1, %4, 0;\n\tsubc.u32 %2, 0, 0;\n\t}"
+      : "=r"(t0), "=r"(t1), "=r"(m)
+      : "r"(r0), "r"(r1), "r"(r3));
+  asm("{\n\tadd.cc.u32 %0, %0, %2;\n\taddc.u32 %1, %1, %3;\n\t}"
+      : "+r"(t0), "+r"(t1)
+      : "r"(m & 1u), "r"(m));
+  uint32_t u0, u1, c;
+  asm("{\n\tsub.cc.u32 %0, 0, %2;\n\tsubc.u32 %1, %2, 0;\n\t}" : "=r"(u0), "=r"(u1) : "r"(r2));
+  asm("{\n\tadd.cc.u32 %0, %0, %3;\n\taddc.cc.u32 %1, %1, %4;\n\taddc.u32 %2, 0, 0;\n\t}"
+      : "+r"(t0), "+r"(t1), "=r"(c)
+      : "r"(u0), "r"(u1));
+  asm("{\n\tadd.cc.u32 %0, %0, %2;\n\taddc.u32 %1, %1, 0;\n\t}" : "+r"(t0), "+r"(t1) : "r"(0u - c));
+  const uint64_t r = ((uint64_t)t1 << 32) | t0;
+  return r >= P ? r - P : r;
+#else
+  return reduce128(a * b, mulhi(a, b));
+#endif
+}
 
 GL_HD uint64_t sqr(uint64_t a) { return mul(a, a); }
 

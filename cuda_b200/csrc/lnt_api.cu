@@ -410,6 +410,11 @@ int lnt_create(uint32_t exponent, uint32_t n, int prp, int device, lnt_test** ou
   }
   lnt::Plan plan;
   if (!lnt::make_plan(n, plan)) return fail(LNT_ERR_UNSUPPORTED_LENGTH, "length must be 2^k, 1 <= k <= 26");
+  if (plan.fast && plan.tile == 8 && lnt::r16_run_words_needed(exponent, plan.log2n) <= 4) {
+    // carry runs of 4 words suffice: narrower column tiles, two CTAs per SM
+    plan.tile = 4;
+    plan.ntiles = plan.n1 / plan.tile;
+  }
   if (n > exponent) return fail(LNT_ERR_UNSUPPORTED_LENGTH, "length exceeds the exponent");
   if ((exponent + n - 1) / n > 30) return fail(LNT_ERR_UNSUPPORTED_LENGTH, "more than 30 bits per word");
   int count = 0;

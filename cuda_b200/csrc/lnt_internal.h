@@ -92,6 +92,7 @@ cudaError_t launch_col_inverse(const TwoPassDesc& d, bool unsigned_mode, cudaStr
 // radix-16 pass variants (lnt_radix16.cu): n2 in [2^6, 2^12], n1 in [2^7, 2^12], n1 >= n2
 bool r16_supported(uint32_t log2n1, uint32_t log2n2);
 uint32_t r16_tile(uint32_t log2n2);
+uint32_t r16_run_words_needed(uint32_t exponent, uint32_t log2n);
 cudaError_t launch_col_forward_r16(const TwoPassDesc& d, bool apply_carries, cudaStream_t s);
 cudaError_t launch_row_square_r16(const TwoPassDesc& d, cudaStream_t s);
 cudaError_t launch_col_inverse_r16(const TwoPassDesc& d, bool unsigned_mode, cudaStream_t s);

@@ -100,11 +100,13 @@ __device__ __forceinline__ void task_square(uint64_t* base, int off) {
 // A pass over `ntrans` transforms of length L; transform g lives at sm + g * ld.
 template <int R, int Mode>  // Mode 0: DIF, 1: DIT, 2: square
 __device__ void pass(uint64_t* sm, int ld, int ntrans, int L, int span, const uint64_t* tw) {
+  // all sizes are powers of two: index arithmetic by shifts and masks
   const int q = span / R, per = L / R, tws = L / span;
+  const int lq = __ffs(q) - 1, lper = __ffs(per) - 1;
   const int total = ntrans * per;
   for (int task = threadIdx.x; task < total; task += blockDim.x) {
-    const int g = task / per, k = task % per;
-    const int b = k / q, t = k % q;
+    const int g = task >> lper, k = task & (per - 1);
+    const int b = k >> lq, t = k & (q - 1);
     uint64_t* base = sm + g * ld;
     if constexpr (Mode == 0)
       task_dif<R>(base, b * span + t, q, t, tw, tws);
@@ -130,76 +132,117 @@ __device__ __forceinline__ void pass_r(int R, uint64_t* sm, int ld, int ntrans, 
 
 constexpr int kRowThreads = 256;
 
-// first pass fused with the HBM read and the 4-step twiddle
+// Forward pass of `rows` row transforms.  The first pass (span = L) reads HBM
+// and applies the 4-step twiddle; later passes read shared memory.  One code
+// body serves both, which keeps the kernel small for the instruction cache.
 template <int R>
-__device__ void row_first_pass(uint64_t* sm, int ld, int rows, int L, const uint64_t* x,
-                               const uint64_t* twf, const uint64_t* twL) {
-  const int q = L / R;
-  for (int task = threadIdx.x; task < rows * q; task += blockDim.x) {
-    const int g = task / q, t = task % q;
-    const size_t rb = (size_t)g * L;
+__device__ void row_dif_pass(uint64_t* sm, int ld, int rows, int L, int span, const uint64_t* x,
+                             const uint64_t* twf, const uint64_t* twL) {
+  const bool first = span == L;
+  const int q = span / R, per = L / R, tws = L / span;
+  const int lq = __ffs(q) - 1, lper = __ffs(per) - 1;
+  for (int task = threadIdx.x; task < rows * per; task += blockDim.x) {
+    const int g = task >> lper, k = task & (per - 1), b = k >> lq, t = k & (q - 1);
+    const int off = b * span + t;
+    uint64_t* base = sm + g * ld;
     uint64_t v[R];
+    if (first) {
+      const size_t rb = (size_t)g * L + off;
 #pragma unroll
-    for (int d = 0; d < R; ++d) v[d] = gl::mul(x[rb + t + q * d], twf[rb + t + q * d]);
+      for (int d = 0; d < R; ++d) v[d] = gl::mul(x[rb + q * d], twf[rb + q * d]);
+    } else {
+#pragma unroll
+      for (int d = 0; d < R; ++d) v[d] = base[sw(off + q * d)];
+    }
     dif<R>(v);
 #pragma unroll
-    for (int r = 0; r < R; ++r) sm[g * ld + sw(t + q * r)] = gl::mul(v[r], twL[t * brev_c<R>(r)]);
+    for (int r = 0; r < R; ++r) {
+      uint64_t y = v[r];
+      if (q > 1) y = gl::mul(y, twL[t * brev_c<R>(r) * tws]);
+      base[sw(off + q * r)] = y;
+    }
   }
 }
 
-// last inverse pass fused with the inverse 4-step twiddle and the HBM write
+// Inverse pass; the last one (span = L) applies the inverse 4-step twiddle and
+// writes HBM.
 template <int R>
-__device__ void row_last_pass(const uint64_t* sm, int ld, int rows, int L, uint64_t* x,
-                              const uint64_t* twi, const uint64_t* itwL) {
-  const int q = L / R;
-  for (int task = threadIdx.x; task < rows * q; task += blockDim.x) {
-    const int g = task / q, t = task % q;
-    const size_t rb = (size_t)g * L;
+__device__ void row_dit_pass(uint64_t* sm, int ld, int rows, int L, int span, uint64_t* x,
+                             const uint64_t* twi, const uint64_t* itwL) {
+  const bool last = span == L;
+  const int q = span / R, per = L / R, tws = L / span;
+  const int lq = __ffs(q) - 1, lper = __ffs(per) - 1;
+  for (int task = threadIdx.x; task < rows * per; task += blockDim.x) {
+    const int g = task >> lper, k = task & (per - 1), b = k >> lq, t = k & (q - 1);
+    const int off = b * span + t;
+    uint64_t* base = sm + g * ld;
     uint64_t v[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = gl::mul(sm[g * ld + sw(t + q * r)], itwL[t * brev_c<R>(r)]);
+    for (int r = 0; r < R; ++r) {
+      uint64_t y = base[sw(off + q * r)];
+      if (q > 1) y = gl::mul(y, itwL[t * brev_c<R>(r) * tws]);
+      v[r] = y;
+    }
     dit_inv<R>(v);
+    if (last) {
+      const size_t rb = (size_t)g * L + off;
 #pragma unroll
-    for (int d = 0; d < R; ++d) x[rb + t + q * d] = gl::mul(v[d], twi[rb + t + q * d]);
+      for (int d = 0; d < R; ++d) x[rb + q * d] = gl::mul(v[d], twi[rb + q * d]);
+    } else {
+#pragma unroll
+      for (int d = 0; d < R; ++d) base[sw(off + q * d)] = v[d];
+    }
   }
 }
 
-__global__ void __launch_bounds__(kRowThreads) row_square_r16(TwoPassDesc D, Passes P, int rows) {
+template <bool Forward>
+__device__ __forceinline__ void row_pass_r(int R, uint64_t* sm, int ld, int rows, int L, int span,
+                                           uint64_t* x, const uint64_t* tw4, const uint64_t* twL) {
+  switch (R) {
+    case 2:
+      if constexpr (Forward) row_dif_pass<2>(sm, ld, rows, L, span, x, tw4, twL);
+      else row_dit_pass<2>(sm, ld, rows, L, span, x, tw4, twL);
+      break;
+    case 4:
+      if constexpr (Forward) row_dif_pass<4>(sm, ld, rows, L, span, x, tw4, twL);
+      else row_dit_pass<4>(sm, ld, rows, L, span, x, tw4, twL);
+      break;
+    case 8:
+      if constexpr (Forward) row_dif_pass<8>(sm, ld, rows, L, span, x, tw4, twL);
+      else row_dit_pass<8>(sm, ld, rows, L, span, x, tw4, twL);
+      break;
+    default:
+      if constexpr (Forward) row_dif_pass<16>(sm, ld, rows, L, span, x, tw4, twL);
+      else row_dit_pass<16>(sm, ld, rows, L, span, x, tw4, twL);
+      break;
+  }
+}
+
+__global__ void __launch_bounds__(kRowThreads, 3) row_square_r16(TwoPassDesc D, Passes P, int rows) {
   extern __shared__ __align__(16) uint64_t sm[];
   const int L = (int)D.n1, ld = padded(L);
   const size_t off = (size_t)blockIdx.x * rows * L;
   uint64_t* x = reinterpret_cast<uint64_t*>(D.x) + off;
-  switch (P.radix[0]) {
-    case 2: row_first_pass<2>(sm, ld, rows, L, x, D.twf + off, D.itw1); break;
-    case 4: row_first_pass<4>(sm, ld, rows, L, x, D.twf + off, D.itw1); break;
-    case 8: row_first_pass<8>(sm, ld, rows, L, x, D.twf + off, D.itw1); break;
-    default: row_first_pass<16>(sm, ld, rows, L, x, D.twf + off, D.itw1); break;
-  }
-  __syncthreads();
-  int span = L / P.radix[0];
-  for (int j = 1; j + 1 < P.m; ++j) {
-    pass_r<0>(P.radix[j], sm, ld, rows, L, span, D.itw1);
+  int span = L;
+  for (int j = 0; j + 1 < P.m; ++j) {
+    row_pass_r<true>(P.radix[j], sm, ld, rows, L, span, x, D.twf + off, D.itw1);
     span /= P.radix[j];
     __syncthreads();
   }
   pass_r<2>(P.radix[P.m - 1], sm, ld, rows, L, span, nullptr);
   __syncthreads();
-  for (int j = P.m - 2; j >= 1; --j) {
+  for (int j = P.m - 2; j >= 0; --j) {
     span *= P.radix[j];
-    pass_r<1>(P.radix[j], sm, ld, rows, L, span, D.iitw1);
-    __syncthreads();
-  }
-  switch (P.radix[0]) {
-    case 2: row_last_pass<2>(sm, ld, rows, L, x, D.twi + off, D.iitw1); break;
-    case 4: row_last_pass<4>(sm, ld, rows, L, x, D.twi + off, D.iitw1); break;
-    case 8: row_last_pass<8>(sm, ld, rows, L, x, D.twi + off, D.iitw1); break;
-    default: row_last_pass<16>(sm, ld, rows, L, x, D.twi + off, D.iitw1); break;
+    row_pass_r<false>(P.radix[j], sm, ld, rows, L, span, x, D.twi + off, D.iitw1);
+    if (j) __syncthreads();
   }
 }
 
 // --------------------------------------------------------------- columns ----
 
-constexpr int kColThreads = 1024;
+// column CTAs: 128 threads per tile column (T = 8: 1024 threads, T = 4: 512)
+template <int T>
+constexpr int col_threads() { return 128 * T; }
 
 // column stride in words: the coalesced staging (lanes = T columns x 32/T
 // rows) then hits distinct banks
@@ -270,7 +313,7 @@ __device__ __forceinline__ void load_widths(const uint8_t* src, unsigned (&out)[
 }
 
 template <int T>
-__global__ void __launch_bounds__(kColThreads) col_forward_r16(TwoPassDesc D, Passes P,
+__global__ void __launch_bounds__(col_threads<T>(), 8 / T) col_forward_r16(TwoPassDesc D, Passes P,
                                                                int apply_carries) {
   extern __shared__ __align__(16) uint64_t sm[];
   const int L = (int)D.n2, ld = col_ld(L, T);
@@ -318,7 +361,7 @@ __global__ void __launch_bounds__(kColThreads) col_forward_r16(TwoPassDesc D, Pa
 }
 
 template <int T>
-__global__ void __launch_bounds__(kColThreads) col_inverse_r16(TwoPassDesc D, Passes P,
+__global__ void __launch_bounds__(col_threads<T>(), 8 / T) col_inverse_r16(TwoPassDesc D, Passes P,
                                                                int unsigned_mode) {
   extern __shared__ __align__(16) uint64_t sm[];
   const int L = (int)D.n2, ld = col_ld(L, T);
@@ -369,6 +412,16 @@ bool r16_supported(uint32_t log2n1, uint32_t log2n2) {
 
 uint32_t r16_tile(uint32_t log2n2) { return log2n2 >= 12 ? 4 : 8; }
 
+// Words a carry run needs: the outgoing carry of a run is below 2^(log2 n + W)
+// in magnitude (W = ceil(q / n)), each word it ripples through takes off at
+// least w_min - 1 bits, and the last word absorbs the remaining +-1.
+uint32_t r16_run_words_needed(uint32_t exponent, uint32_t log2n) {
+  const uint32_t n = 1u << log2n;
+  const uint32_t wmax = (exponent + n - 1) / n, wmin = exponent / n;
+  if (wmin < 3) return 64;
+  return (log2n + wmax + wmin - 2) / (wmin - 1) + 1;
+}
+
 cudaError_t launch_row_square_r16(const TwoPassDesc& d, cudaStream_t s) {
   const int L = (int)d.n1, rows = row_rows_per_cta(L, (int)d.n2);
   const size_t smem = (size_t)rows * padded(L) * 8;
@@ -385,7 +438,7 @@ cudaError_t col_forward_t(const TwoPassDesc& d, bool apply, cudaStream_t s) {
   cudaError_t e = cudaFuncSetAttribute(col_forward_r16<T>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  col_forward_r16<T><<<d.ntiles, kColThreads, smem, s>>>(d, make_passes((int)d.log2n2), apply ? 1 : 0);
+  col_forward_r16<T><<<d.ntiles, col_threads<T>(), smem, s>>>(d, make_passes((int)d.log2n2), apply ? 1 : 0);
   return cudaGetLastError();
 }
 
@@ -395,7 +448,7 @@ cudaError_t col_inverse_t(const TwoPassDesc& d, bool unsigned_mode, cudaStream_t
   cudaError_t e = cudaFuncSetAttribute(col_inverse_r16<T>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  col_inverse_r16<T><<<d.ntiles, kColThreads, smem, s>>>(d, make_passes((int)d.log2n2),
+  col_inverse_r16<T><<<d.ntiles, col_threads<T>(), smem, s>>>(d, make_passes((int)d.log2n2),
                                                          unsigned_mode ? 1 : 0);
   return cudaGetLastError();
 }
