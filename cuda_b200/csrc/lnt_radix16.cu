@@ -218,7 +218,7 @@ __device__ __forceinline__ void row_pass_r(int R, uint64_t* sm, int ld, int rows
   }
 }
 
-__global__ void __launch_bounds__(kRowThreads, 3) row_square_r16(TwoPassDesc D, Passes P, int rows) {
+__global__ void __launch_bounds__(kRowThreads, 4) row_square_r16(TwoPassDesc D, Passes P, int rows) {
   extern __shared__ __align__(16) uint64_t sm[];
   const int L = (int)D.n1, ld = padded(L);
   const size_t off = (size_t)blockIdx.x * rows * L;
@@ -398,7 +398,7 @@ __global__ void __launch_bounds__(col_threads<T>(), 8 / T) col_inverse_r16(TwoPa
 }
 
 int row_rows_per_cta(int L, int n2) {
-  int rows = 8192 / L;
+  int rows = 4096 / L;
   if (rows < 1) rows = 1;
   while (rows > 1 && n2 / rows < 148) rows /= 2;
   return rows;
