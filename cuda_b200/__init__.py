@@ -4,6 +4,7 @@ The product is liblucasntt.so (CUDA for sm_100a behind the C ABI in
 include/lucasntt.h); this package is its Python binding.
 """
 from .api import (  # noqa: F401
+    Batch,
     LucasNTTError,
     LucasTest,
     check_provided_length,
@@ -11,4 +12,5 @@ from .api import (  # noqa: F401
     lib,
     parse_length,
     secured_log2_length,
+    test_device_bytes,
 )

@@ -34,6 +34,13 @@ class KernelTime(ctypes.Structure):
                 ("total_ms", ctypes.c_float)]
 
 
+class BatchResult(ctypes.Structure):
+    """lnt_batch_result."""
+    _fields_ = [("id", ctypes.c_uint64), ("iterations", ctypes.c_uint64), ("res64", ctypes.c_uint64),
+                ("seconds", ctypes.c_double), ("exponent", ctypes.c_uint32), ("n", ctypes.c_uint32),
+                ("prp", ctypes.c_int), ("is_prime", ctypes.c_int), ("status", ctypes.c_int)]
+
+
 class LucasNTTError(RuntimeError):
     def __init__(self, status: int, where: str):
         L = lib()
@@ -75,6 +82,13 @@ def lib() -> ctypes.CDLL:
         "lnt_set_stream": ([vp, vp], i32),
         "lnt_synchronize": ([vp], i32),
         "lnt_profile_iterations": ([vp, u64, ctypes.POINTER(KernelTime), i32, ctypes.POINTER(i32)], i32),
+        "lnt_test_device_bytes": ([u32, u32], u64),
+        "lnt_batch_create": ([i32, u64, ctypes.POINTER(vp)], i32),
+        "lnt_batch_destroy": ([vp], i32),
+        "lnt_batch_submit": ([vp, u32, u32, i32, u64, ctypes.POINTER(u64)], i32),
+        "lnt_batch_run": ([vp, u64], i32),
+        "lnt_batch_poll": ([vp, ctypes.POINTER(BatchResult), i32, ctypes.POINTER(i32)], i32),
+        "lnt_batch_status": ([vp, ctypes.POINTER(u32), ctypes.POINTER(u64)], i32),
     }
     for name, (args, res) in sigs.items():
         f = getattr(L, name)
@@ -204,3 +218,66 @@ class LucasTest:
                "lnt_profile_iterations")
         return {arr[i].name.decode(): (int(arr[i].launches), float(arr[i].total_ms))
                 for i in range(min(cap, count.value))}
+
+
+def test_device_bytes(exponent: int, n: int = 0) -> int:
+    """Device bytes one test occupies (the batch engine's budget unit)."""
+    return int(lib().lnt_test_device_bytes(exponent, n))
+
+
+class Batch:
+    """Many LL / PRP tests on one GPU, admitted under an HBM budget and retired
+    as they finish (lnt_batch_*)."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0):
+        h = ctypes.c_void_p()
+        _check(lib().lnt_batch_create(device, int(hbm_budget_bytes), ctypes.byref(h)), "lnt_batch_create")
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().lnt_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def submit(self, exponent: int, n: int = 0, prp: bool = False, iterations: int = 0):
+        """Admit a test; returns its id, or None when it does not fit the budget."""
+        i = ctypes.c_uint64()
+        st = lib().lnt_batch_submit(self._h, exponent, n, int(bool(prp)), int(iterations), ctypes.byref(i))
+        if st == LNT_ERR_BUDGET:
+            return None
+        _check(st, "lnt_batch_submit")
+        return int(i.value)
+
+    def run(self, iterations: int) -> None:
+        _check(lib().lnt_batch_run(self._h, int(iterations)), "lnt_batch_run")
+
+    def poll(self) -> list[dict]:
+        out = []
+        buf = (BatchResult * 64)()
+        while True:
+            c = ctypes.c_int()
+            _check(lib().lnt_batch_poll(self._h, buf, 64, ctypes.byref(c)), "lnt_batch_poll")
+            for k in range(c.value):
+                r = buf[k]
+                out.append({"id": r.id, "exponent": r.exponent, "n": r.n, "prp": bool(r.prp),
+                            "iterations": r.iterations, "res64": r.res64, "is_prime": bool(r.is_prime),
+                            "status": r.status, "seconds": r.seconds})
+            if c.value < 64:
+                return out
+
+    def status(self) -> tuple[int, int]:
+        a, b = ctypes.c_uint32(), ctypes.c_uint64()
+        _check(lib().lnt_batch_status(self._h, ctypes.byref(a), ctypes.byref(b)), "lnt_batch_status")
+        return int(a.value), int(b.value)

@@ -35,6 +35,7 @@ struct lnt_test {
   uint64_t* rt = nullptr;
   uint64_t* irt = nullptr;
   lnt::ResidentDesc* rdesc = nullptr;
+  lnt::TwoPassDesc* tdesc = nullptr;  // device copy of the two-pass descriptor
   // two-pass plan
   uint64_t *twf = nullptr, *twi = nullptr;
   uint64_t *rt1 = nullptr, *irt1 = nullptr, *rt2 = nullptr, *irt2 = nullptr;
@@ -96,7 +97,7 @@ cudaError_t dalloc(T** p, size_t count) {
 }
 
 void free_all(lnt_test* t) {
-  void* ptrs[] = {t->x, t->w, t->uw, t->widths, t->status, t->rt, t->irt, t->rdesc,
+  void* ptrs[] = {t->x, t->w, t->uw, t->widths, t->status, t->rt, t->irt, t->rdesc, t->tdesc,
                   t->twf, t->twi, t->rt1, t->irt1, t->rt2, t->irt2, t->itw1, t->iitw1,
                   t->itw2, t->iitw2, t->wt, t->uwt, t->widt, t->carry, t->canon,
                   t->blk_carry, t->blk_fn, t->blk_cin, t->cflags};
@@ -356,9 +357,11 @@ int queue_iterations(lnt_test* t, uint64_t iterations, LaunchTimer* timer) {
     lnt::TwoPassDesc d = twopass_desc(t);
     for (uint64_t i = 0; i < iterations; ++i) {
       if (t->plan.fast) {
-        LNT_LAUNCH(lnt::launch_col_forward_r16(d, t->pending_carries, t->stream), "col_forward");
-        LNT_LAUNCH(lnt::launch_row_square_r16(d, t->stream), "row_square");
-        LNT_LAUNCH(lnt::launch_col_inverse_r16(d, t->canonical_input, t->stream), "col_inverse");
+        LNT_LAUNCH(lnt::launch_col_forward_r16(d, t->tdesc, 1, t->pending_carries, t->stream),
+                   "col_forward");
+        LNT_LAUNCH(lnt::launch_row_square_r16(d, t->tdesc, 1, t->stream), "row_square");
+        LNT_LAUNCH(lnt::launch_col_inverse_r16(d, t->tdesc, 1, t->canonical_input, t->stream),
+                   "col_inverse");
       } else {
         LNT_LAUNCH(lnt::launch_col_forward(d, t->pending_carries, t->stream), "col_forward");
         LNT_LAUNCH(lnt::launch_row_square(d, t->stream), "row_square");
@@ -379,6 +382,54 @@ int queue_iterations(lnt_test* t, uint64_t iterations, LaunchTimer* timer) {
 namespace lnt {
 // Lets other translation units of the library report a failure detail.
 void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+// ---- hooks for the batch engine (lnt_batch.cu) -----------------------------
+const Plan& test_plan(const lnt_test* t) { return t->plan; }
+int test_prp(const lnt_test* t) { return t->prp; }
+const TwoPassDesc* test_twopass_device_desc(const lnt_test* t) { return t->tdesc; }
+TwoPassDesc test_twopass_desc(const lnt_test* t) { return twopass_desc(t); }
+bool test_ready_for_group(const lnt_test* t) {
+  // batched two-pass launches assume the steady state: carries pending, signed outputs
+  return t->plan.kind == PlanKind::Resident || (t->pending_carries && !t->canonical_input);
+}
+ResidentDesc test_resident_desc(const lnt_test* t, uint64_t iterations) {
+  ResidentDesc d{};
+  d.digits = t->x;
+  d.w = t->w;
+  d.uw = t->uw;
+  d.widths = t->widths;
+  d.rt = t->rt;
+  d.irt = t->irt;
+  d.status = t->status;
+  d.n = t->n;
+  d.log2n = t->plan.log2n;
+  d.prp = (uint32_t)t->prp;
+  d.unsigned_first = t->canonical_input ? 1 : 0;
+  d.iterations = iterations;
+  return d;
+}
+// bookkeeping after squarings were launched outside lnt_iterate
+void test_mark_iterated(lnt_test* t) {
+  if (t->plan.kind == PlanKind::TwoPass) t->pending_carries = true;
+  t->canonical_input = false;
+  t->pristine = false;
+  t->canon_valid = false;
+}
+
+// Device bytes lnt_create allocates for a test (the batch engine's budget unit).
+uint64_t test_device_bytes(uint32_t n) {
+  Plan plan;
+  if (!make_plan(n, plan)) return 0;
+  const uint64_t nb = n / canon_block_size(n);
+  uint64_t b = 8ull * n * 4 + n + 4 + nb * 10 + 4;  // x, w, uw, canon, widths, status, readout
+  if (plan.kind == PlanKind::Resident) {
+    b += 8ull * n + sizeof(ResidentDesc);  // root tables
+  } else {
+    b += 16ull * n + 8ull * (plan.n1 + plan.n2) + 8ull * plan.ntiles * plan.n2 + sizeof(TwoPassDesc);
+    if (plan.fast) b += 16ull * (plan.n1 + plan.n2) + 17ull * n;  // inner twiddles, tile-major tables
+  }
+  return b;
+}
 }  // namespace lnt
 
 extern "C" {
@@ -477,6 +528,17 @@ int lnt_create(uint32_t exponent, uint32_t n, int prp, int device, lnt_test** ou
       return bail(cuda_fail(e, "allocate twiddles"));
     if ((e = lnt::launch_twiddles(plan.n1, plan.n2, plan.log2n2, t->twf, t->twi, t->stream)))
       return bail(cuda_fail(e, "twiddles"));
+    // the device copy of the descriptor, built once every buffer it names exists
+    const lnt::TwoPassDesc hd = twopass_desc(t);
+    const void* needed[] = {hd.x, hd.carry, hd.w, hd.uw, hd.widths, hd.twf, hd.twi, hd.rt1,
+                            hd.irt1, hd.rt2, hd.irt2, hd.status};
+    for (const void* ptr : needed)
+      if (!ptr) return bail(fail(LNT_ERR_CUDA, "internal: descriptor built before its buffers"));
+    if (plan.fast && (!hd.itw1 || !hd.iitw1 || !hd.itw2 || !hd.iitw2 || !hd.wt || !hd.uwt || !hd.widt))
+      return bail(fail(LNT_ERR_CUDA, "internal: descriptor built before its buffers"));
+    if ((e = dalloc(&t->tdesc, 1)) ||
+        (e = cudaMemcpy(t->tdesc, &hd, sizeof(hd), cudaMemcpyHostToDevice)))
+      return bail(cuda_fail(e, "descriptor"));
   }
   if ((e = cudaStreamSynchronize(t->stream))) return bail(cuda_fail(e, "initialize"));
   if ((st = lnt_init_test(t)) != LNT_OK) return bail(st);

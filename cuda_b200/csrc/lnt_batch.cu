@@ -1,0 +1,330 @@
+// Batch engine: many independent LL / PRP tests of mixed lengths on one GPU.
+//
+// The reference runs one exponent per process (main_process.cu:64-149 builds
+// one MainProcess, lucas_prp.cu drives one residue).  Here tests are grouped
+// by length and every group advances with batched launches: each kernel of
+// the squaring takes a device array of test descriptors and blockIdx.y picks
+// the test, so one launch per kernel covers all tests of a length.  The
+// SMEM-resident plan (n <= 4096) runs all its tests, of any lengths, in one
+// launch with one CTA per test and a per-test iteration count.  Groups run on
+// their own streams so small groups overlap.  Tests are admitted against an
+// HBM budget and retired (Res64 and verdict recorded, memory released) as they
+// finish, so a caller can keep the engine full: continuous batching.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <deque>
+#include <map>
+#include <vector>
+
+#include "../../include/lucasntt.h"
+#include "lnt_internal.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Entry {
+  uint64_t id;
+  lnt_test* t;
+  uint32_t q, n;
+  int prp;
+  uint64_t target, done;
+  uint64_t bytes;
+  Clock::time_point submitted;
+};
+
+struct Group {
+  uint32_t n = 0;
+  std::vector<size_t> members;  // indices into active
+  lnt::TwoPassDesc geometry{};
+  lnt::TwoPassDesc* d_descs = nullptr;
+  size_t cap = 0;
+  cudaStream_t stream = nullptr;
+};
+
+int berr(int status, const std::string& msg) {
+  lnt::set_last_error(msg);
+  return status;
+}
+
+}  // namespace
+
+struct lnt_batch {
+  int device = 0;
+  uint64_t budget = 0, used = 0;
+  uint64_t next_id = 1;
+  cudaStream_t stream = nullptr;
+  std::vector<Entry> active;
+  std::deque<lnt_batch_result> finished;
+  // launch groups, rebuilt when membership changes
+  bool dirty = true;
+  std::map<uint64_t, Group> groups;  // fast two-pass tests by (length, tile width)
+  std::vector<size_t> resident;      // SMEM-resident tests
+  std::vector<size_t> singles;       // tests iterated one by one
+  lnt::ResidentDesc* d_rdescs = nullptr;
+  size_t rcap = 0;
+  std::vector<cudaStream_t> spare_streams;
+};
+
+namespace {
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+#define BCUDA(call, what)                                                          \
+  do {                                                                             \
+    cudaError_t e_ = (call);                                                       \
+    if (e_ != cudaSuccess) return berr(LNT_ERR_CUDA, std::string(what) + ": " +    \
+                                                         cudaGetErrorString(e_)); \
+  } while (0)
+
+cudaStream_t take_stream(lnt_batch* b) {
+  if (!b->spare_streams.empty()) {
+    cudaStream_t s = b->spare_streams.back();
+    b->spare_streams.pop_back();
+    return s;
+  }
+  cudaStream_t s = nullptr;
+  cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  return s;
+}
+
+int rebuild(lnt_batch* b) {
+  for (auto& kv : b->groups) {
+    if (kv.second.d_descs) cudaFree(kv.second.d_descs);
+    b->spare_streams.push_back(kv.second.stream);
+  }
+  b->groups.clear();
+  b->resident.clear();
+  b->singles.clear();
+  for (size_t i = 0; i < b->active.size(); ++i) {
+    const lnt::Plan& p = lnt::test_plan(b->active[i].t);
+    if (p.kind == lnt::PlanKind::Resident) {
+      b->resident.push_back(i);
+    } else if (p.fast && lnt::test_ready_for_group(b->active[i].t)) {
+      // one launch serves tests of identical geometry: same length and tile width
+      Group& g = b->groups[((uint64_t)p.n << 8) | p.tile];
+      g.n = p.n;
+      g.members.push_back(i);
+    } else {
+      b->singles.push_back(i);
+    }
+  }
+  for (auto& kv : b->groups) {
+    Group& g = kv.second;
+    std::vector<lnt::TwoPassDesc> h;
+    for (size_t i : g.members) h.push_back(lnt::test_twopass_desc(b->active[i].t));
+    g.geometry = h[0];
+    BCUDA(cudaMalloc((void**)&g.d_descs, h.size() * sizeof(lnt::TwoPassDesc)), "group descriptors");
+    g.cap = h.size();
+    BCUDA(cudaMemcpy(g.d_descs, h.data(), h.size() * sizeof(lnt::TwoPassDesc), cudaMemcpyHostToDevice),
+          "upload descriptors");
+    g.stream = take_stream(b);
+  }
+  if (b->resident.size() > b->rcap) {
+    if (b->d_rdescs) cudaFree(b->d_rdescs);
+    b->rcap = std::max<size_t>(b->resident.size(), 2 * b->rcap);
+    BCUDA(cudaMalloc((void**)&b->d_rdescs, b->rcap * sizeof(lnt::ResidentDesc)), "resident descriptors");
+  }
+  b->dirty = false;
+  return LNT_OK;
+}
+
+int retire_finished(lnt_batch* b) {
+  bool any = false;
+  for (size_t i = 0; i < b->active.size();) {
+    Entry& e = b->active[i];
+    if (e.done < e.target) {
+      ++i;
+      continue;
+    }
+    lnt_batch_result r{};
+    r.id = e.id;
+    r.exponent = e.q;
+    r.n = e.n;
+    r.prp = e.prp;
+    r.iterations = e.done;
+    int st = lnt_res64(e.t, &r.res64);
+    if (st == LNT_OK) st = lnt_is_prime(e.t, &r.is_prime);
+    r.status = st;
+    r.seconds = std::chrono::duration<double>(Clock::now() - e.submitted).count();
+    b->finished.push_back(r);
+    lnt_destroy(e.t);
+    b->used -= e.bytes;
+    b->active.erase(b->active.begin() + (long)i);
+    any = true;
+  }
+  if (any) b->dirty = true;
+  return LNT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint64_t lnt_test_device_bytes(uint32_t exponent, uint32_t n) {
+  if (n == 0) n = 1u << lnt_secured_log2_length(exponent);
+  return lnt::test_device_bytes(n);
+}
+
+int lnt_batch_create(int device, uint64_t hbm_budget_bytes, lnt_batch** out) {
+  if (!out) return berr(LNT_ERR_INVALID_ARGUMENT, "null output pointer");
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+    return berr(LNT_ERR_NO_DEVICE, "no CUDA device");
+  if (device < 0 || device >= count) return berr(LNT_ERR_INVALID_ARGUMENT, "bad device index");
+  DeviceGuard guard(device);
+  lnt_batch* b = new lnt_batch();
+  b->device = device;
+  b->budget = hbm_budget_bytes;
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete b;
+    return berr(LNT_ERR_CUDA, "cudaStreamCreate");
+  }
+  *out = b;
+  return LNT_OK;
+}
+
+int lnt_batch_destroy(lnt_batch* b) {
+  if (!b) return LNT_OK;
+  DeviceGuard guard(b->device);
+  cudaDeviceSynchronize();
+  for (auto& e : b->active) lnt_destroy(e.t);
+  for (auto& kv : b->groups) {
+    if (kv.second.d_descs) cudaFree(kv.second.d_descs);
+    if (kv.second.stream) cudaStreamDestroy(kv.second.stream);
+  }
+  for (cudaStream_t s : b->spare_streams)
+    if (s) cudaStreamDestroy(s);
+  if (b->d_rdescs) cudaFree(b->d_rdescs);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return LNT_OK;
+}
+
+int lnt_batch_submit(lnt_batch* b, uint32_t exponent, uint32_t n, int prp, uint64_t iterations,
+                     uint64_t* id) {
+  if (!b) return berr(LNT_ERR_INVALID_ARGUMENT, "null batch");
+  DeviceGuard guard(b->device);
+  if (n == 0) n = 1u << lnt_secured_log2_length(exponent);
+  const uint64_t bytes = lnt::test_device_bytes(n);
+  if (bytes == 0) return berr(LNT_ERR_UNSUPPORTED_LENGTH, "unsupported length");
+  if (b->budget && b->used + bytes > b->budget)
+    return berr(LNT_ERR_BUDGET, "test does not fit the HBM budget");
+  lnt_test* t = nullptr;
+  int st = lnt_create(exponent, n, prp, b->device, &t);
+  if (st != LNT_OK) return st;
+  Entry e{};
+  e.id = b->next_id++;
+  e.t = t;
+  e.q = exponent;
+  e.n = n;
+  e.prp = prp ? 1 : 0;
+  e.target = iterations ? iterations : (prp ? (uint64_t)exponent : (uint64_t)exponent - 2);
+  e.done = 0;
+  e.bytes = bytes;
+  e.submitted = Clock::now();
+  const lnt::Plan& p = lnt::test_plan(t);
+  if (p.kind == lnt::PlanKind::TwoPass && e.target > 0) {
+    // the first squaring reads non-negative digits (unsigned outputs): run it
+    // alone, after which the test joins its length group
+    if ((st = lnt_iterate(t, 1)) != LNT_OK || (st = lnt_synchronize(t)) != LNT_OK) {
+      lnt_destroy(t);
+      return st;
+    }
+    e.done = 1;
+  }
+  b->used += bytes;
+  b->active.push_back(e);
+  b->dirty = true;
+  if (id) *id = e.id;
+  return retire_finished(b);
+}
+
+int lnt_batch_run(lnt_batch* b, uint64_t iterations) {
+  if (!b) return berr(LNT_ERR_INVALID_ARGUMENT, "null batch");
+  DeviceGuard guard(b->device);
+  if (b->active.empty() || iterations == 0) return LNT_OK;
+  int st;
+  if (b->dirty && (st = rebuild(b)) != LNT_OK) return st;
+  // grouped tests advance in lockstep: no test of a group may pass its target
+  uint64_t k = iterations;
+  for (auto& kv : b->groups)
+    for (size_t i : kv.second.members) k = std::min(k, b->active[i].target - b->active[i].done);
+  // SMEM-resident tests: one launch, per-test counts
+  if (!b->resident.empty()) {
+    std::vector<lnt::ResidentDesc> h;
+    uint32_t max_n = 0;
+    for (size_t i : b->resident) {
+      Entry& e = b->active[i];
+      h.push_back(lnt::test_resident_desc(e.t, std::min(iterations, e.target - e.done)));
+      max_n = std::max(max_n, e.n);
+    }
+    BCUDA(cudaMemcpyAsync(b->d_rdescs, h.data(), h.size() * sizeof(lnt::ResidentDesc),
+                          cudaMemcpyHostToDevice, b->stream),
+          "upload resident descriptors");
+    BCUDA(lnt::launch_resident(b->d_rdescs, (uint32_t)h.size(), max_n, b->stream), "resident kernel");
+  }
+  for (auto& kv : b->groups) {
+    Group& g = kv.second;
+    const uint32_t cnt = (uint32_t)g.members.size();
+    for (uint64_t it = 0; it < k; ++it) {
+      BCUDA(lnt::launch_col_forward_r16(g.geometry, g.d_descs, cnt, true, g.stream), "col_forward");
+      BCUDA(lnt::launch_row_square_r16(g.geometry, g.d_descs, cnt, g.stream), "row_square");
+      BCUDA(lnt::launch_col_inverse_r16(g.geometry, g.d_descs, cnt, false, g.stream), "col_inverse");
+    }
+  }
+  for (size_t i : b->singles) {
+    Entry& e = b->active[i];
+    const uint64_t ki = std::min(iterations, e.target - e.done);
+    if ((st = lnt_iterate(e.t, ki)) != LNT_OK) return st;
+  }
+  BCUDA(cudaDeviceSynchronize(), "synchronize");
+  for (size_t i : b->resident) {
+    Entry& e = b->active[i];
+    e.done += std::min(iterations, e.target - e.done);
+    lnt::test_mark_iterated(e.t);
+  }
+  for (auto& kv : b->groups)
+    for (size_t i : kv.second.members) {
+      b->active[i].done += k;
+      lnt::test_mark_iterated(b->active[i].t);
+    }
+  for (size_t i : b->singles) {
+    Entry& e = b->active[i];
+    e.done += std::min(iterations, e.target - e.done);
+  }
+  return retire_finished(b);
+}
+
+int lnt_batch_poll(lnt_batch* b, lnt_batch_result* out, int cap, int* count) {
+  if (!b || !count || (cap > 0 && !out)) return berr(LNT_ERR_INVALID_ARGUMENT, "null argument");
+  int k = 0;
+  while (k < cap && !b->finished.empty()) {
+    out[k++] = b->finished.front();
+    b->finished.pop_front();
+  }
+  *count = k;
+  return LNT_OK;
+}
+
+int lnt_batch_status(lnt_batch* b, uint32_t* active, uint64_t* bytes_in_use) {
+  if (!b) return berr(LNT_ERR_INVALID_ARGUMENT, "null batch");
+  if (active) *active = (uint32_t)b->active.size();
+  if (bytes_in_use) *bytes_in_use = b->used;
+  return LNT_OK;
+}
+
+}  // extern "C"

@@ -93,9 +93,14 @@ cudaError_t launch_col_inverse(const TwoPassDesc& d, bool unsigned_mode, cudaStr
 bool r16_supported(uint32_t log2n1, uint32_t log2n2);
 uint32_t r16_tile(uint32_t log2n2);
 uint32_t r16_run_words_needed(uint32_t exponent, uint32_t log2n);
-cudaError_t launch_col_forward_r16(const TwoPassDesc& d, bool apply_carries, cudaStream_t s);
-cudaError_t launch_row_square_r16(const TwoPassDesc& d, cudaStream_t s);
-cudaError_t launch_col_inverse_r16(const TwoPassDesc& d, bool unsigned_mode, cudaStream_t s);
+// `d` gives the geometry (shared by every test of the launch); `dd` is a device
+// array of `count` descriptors of tests with that geometry (blockIdx.y picks one).
+cudaError_t launch_col_forward_r16(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
+                                   bool apply_carries, cudaStream_t s);
+cudaError_t launch_row_square_r16(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
+                                  cudaStream_t s);
+cudaError_t launch_col_inverse_r16(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
+                                   bool unsigned_mode, cudaStream_t s);
 
 // ------------------------------------------------------------- tables ----
 cudaError_t launch_weights(uint32_t exponent, uint32_t n, uint64_t* w, uint64_t* uw,
@@ -130,4 +135,19 @@ uint32_t canon_block_size(uint32_t n);
 cudaError_t launch_canonicalize(const CanonDesc& d, cudaStream_t s);
 cudaError_t launch_fill_max(uint64_t* out, const uint8_t* widths, uint32_t n, cudaStream_t s);
 
+// ------------------------------------------- hooks for the batch engine ----
+}  // namespace lnt
+
+struct lnt_test;
+
+namespace lnt {
+const Plan& test_plan(const lnt_test* t);
+int test_prp(const lnt_test* t);
+const TwoPassDesc* test_twopass_device_desc(const lnt_test* t);
+TwoPassDesc test_twopass_desc(const lnt_test* t);
+bool test_ready_for_group(const lnt_test* t);
+ResidentDesc test_resident_desc(const lnt_test* t, uint64_t iterations);
+void test_mark_iterated(lnt_test* t);
+uint64_t test_device_bytes(uint32_t n);
+void set_last_error(const std::string& msg);
 }  // namespace lnt

@@ -218,8 +218,9 @@ __device__ __forceinline__ void row_pass_r(int R, uint64_t* sm, int ld, int rows
   }
 }
 
-__global__ void __launch_bounds__(kRowThreads, 4) row_square_r16(TwoPassDesc D, Passes P, int rows) {
+__global__ void __launch_bounds__(kRowThreads, 4) row_square_r16(const TwoPassDesc* __restrict__ Ds, Passes P, int rows) {
   extern __shared__ __align__(16) uint64_t sm[];
+  const TwoPassDesc& D = Ds[blockIdx.y];
   const int L = (int)D.n1, ld = padded(L);
   const size_t off = (size_t)blockIdx.x * rows * L;
   uint64_t* x = reinterpret_cast<uint64_t*>(D.x) + off;
@@ -313,9 +314,10 @@ __device__ __forceinline__ void load_widths(const uint8_t* src, unsigned (&out)[
 }
 
 template <int T>
-__global__ void __launch_bounds__(col_threads<T>(), 8 / T) col_forward_r16(TwoPassDesc D, Passes P,
-                                                               int apply_carries) {
+__global__ void __launch_bounds__(col_threads<T>(), 8 / T) col_forward_r16(const TwoPassDesc* __restrict__ Ds,
+                                                                      Passes P, int apply_carries) {
   extern __shared__ __align__(16) uint64_t sm[];
+  const TwoPassDesc& D = Ds[blockIdx.y];
   const int L = (int)D.n2, ld = col_ld(L, T);
   const uint32_t n1 = D.n1, t0 = blockIdx.x, c0 = t0 * T;
   uint32_t status = 0;
@@ -361,9 +363,10 @@ __global__ void __launch_bounds__(col_threads<T>(), 8 / T) col_forward_r16(TwoPa
 }
 
 template <int T>
-__global__ void __launch_bounds__(col_threads<T>(), 8 / T) col_inverse_r16(TwoPassDesc D, Passes P,
-                                                               int unsigned_mode) {
+__global__ void __launch_bounds__(col_threads<T>(), 8 / T) col_inverse_r16(const TwoPassDesc* __restrict__ Ds,
+                                                                      Passes P, int unsigned_mode) {
   extern __shared__ __align__(16) uint64_t sm[];
+  const TwoPassDesc& D = Ds[blockIdx.y];
   const int L = (int)D.n2, ld = col_ld(L, T);
   const uint32_t n1 = D.n1, t0 = blockIdx.x, c0 = t0 * T;
 
@@ -422,43 +425,52 @@ uint32_t r16_run_words_needed(uint32_t exponent, uint32_t log2n) {
   return (log2n + wmax + wmin - 2) / (wmin - 1) + 1;
 }
 
-cudaError_t launch_row_square_r16(const TwoPassDesc& d, cudaStream_t s) {
+cudaError_t launch_row_square_r16(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
+                                  cudaStream_t s) {
   const int L = (int)d.n1, rows = row_rows_per_cta(L, (int)d.n2);
   const size_t smem = (size_t)rows * padded(L) * 8;
   cudaError_t e = cudaFuncSetAttribute(row_square_r16, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return e;
-  row_square_r16<<<d.n2 / rows, kRowThreads, smem, s>>>(d, make_passes((int)d.log2n1), rows);
+  row_square_r16<<<dim3(d.n2 / rows, count), kRowThreads, smem, s>>>(dd, make_passes((int)d.log2n1),
+                                                                     rows);
   return cudaGetLastError();
 }
 
 template <int T>
-cudaError_t col_forward_t(const TwoPassDesc& d, bool apply, cudaStream_t s) {
+cudaError_t col_forward_t(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count, bool apply,
+                          cudaStream_t s) {
   const size_t smem = (size_t)T * col_ld((int)d.n2, T) * 8;
   cudaError_t e = cudaFuncSetAttribute(col_forward_r16<T>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  col_forward_r16<T><<<d.ntiles, col_threads<T>(), smem, s>>>(d, make_passes((int)d.log2n2), apply ? 1 : 0);
+  col_forward_r16<T><<<dim3(d.ntiles, count), col_threads<T>(), smem, s>>>(
+      dd, make_passes((int)d.log2n2), apply ? 1 : 0);
   return cudaGetLastError();
 }
 
 template <int T>
-cudaError_t col_inverse_t(const TwoPassDesc& d, bool unsigned_mode, cudaStream_t s) {
+cudaError_t col_inverse_t(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
+                          bool unsigned_mode, cudaStream_t s) {
   const size_t smem = (size_t)T * col_ld((int)d.n2, T) * 8;
   cudaError_t e = cudaFuncSetAttribute(col_inverse_r16<T>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  col_inverse_r16<T><<<d.ntiles, col_threads<T>(), smem, s>>>(d, make_passes((int)d.log2n2),
-                                                         unsigned_mode ? 1 : 0);
+  col_inverse_r16<T><<<dim3(d.ntiles, count), col_threads<T>(), smem, s>>>(
+      dd, make_passes((int)d.log2n2), unsigned_mode ? 1 : 0);
   return cudaGetLastError();
 }
 
-cudaError_t launch_col_forward_r16(const TwoPassDesc& d, bool apply, cudaStream_t s) {
-  return d.tile == 4 ? col_forward_t<4>(d, apply, s) : col_forward_t<8>(d, apply, s);
+cudaError_t launch_col_forward_r16(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
+                                   bool apply, cudaStream_t s) {
+  return d.tile == 4 ? col_forward_t<4>(d, dd, count, apply, s)
+                     : col_forward_t<8>(d, dd, count, apply, s);
 }
 
-cudaError_t launch_col_inverse_r16(const TwoPassDesc& d, bool unsigned_mode, cudaStream_t s) {
-  return d.tile == 4 ? col_inverse_t<4>(d, unsigned_mode, s) : col_inverse_t<8>(d, unsigned_mode, s);
+cudaError_t launch_col_inverse_r16(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
+                                   bool unsigned_mode, cudaStream_t s) {
+  return d.tile == 4 ? col_inverse_t<4>(d, dd, count, unsigned_mode, s)
+                     : col_inverse_t<8>(d, dd, count, unsigned_mode, s);
 }
 
 }  // namespace lnt

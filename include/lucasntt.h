@@ -132,6 +132,51 @@ typedef struct lnt_kernel_time {
 int lnt_profile_iterations(lnt_test* t, uint64_t iterations, lnt_kernel_time* out, int cap,
                            int* count);
 
+/* ---- batches of tests ------------------------------------------------------ */
+
+/* The reference runs one exponent per process (main_process.cu:64-149); per
+ * test it is LucasPRP (lucas_prp.cu:24-229).  A batch runs many independent
+ * LL / PRP tests of mixed lengths on one GPU: tests of a length share batched
+ * launches, tests are admitted against an HBM budget and retired as they
+ * finish (continuous batching).  Results are bit-identical to running each
+ * test alone. */
+typedef struct lnt_batch lnt_batch;
+
+typedef struct lnt_batch_result {
+  uint64_t id;         /* as returned by lnt_batch_submit */
+  uint64_t iterations; /* squarings performed */
+  uint64_t res64;      /* Res64 of the final residue */
+  double seconds;      /* submission to completion, host clock */
+  uint32_t exponent;
+  uint32_t n;
+  int prp;
+  int is_prime;        /* residue 0 (LL) / 9 (PRP): meaningful for full tests */
+  int status;          /* LNT_OK, or the readout's error */
+} lnt_batch_result;
+
+/* Device bytes one test of exponent q at length n (0 = policy) occupies. */
+uint64_t lnt_test_device_bytes(uint32_t exponent, uint32_t n);
+
+/* hbm_budget_bytes = 0: no budget. */
+int lnt_batch_create(int device, uint64_t hbm_budget_bytes, lnt_batch** out);
+int lnt_batch_destroy(lnt_batch* b);
+
+/* Admit a test (n = 0: policy length; iterations = 0: the full test, q - 2
+ * squarings for LL and q for PRP as lucas_prp.cu:167).  LNT_ERR_BUDGET when it
+ * does not fit the budget now. */
+int lnt_batch_submit(lnt_batch* b, uint32_t exponent, uint32_t n, int prp, uint64_t iterations,
+                     uint64_t* id);
+
+/* Advance every admitted test by up to `iterations` squarings (none passes its
+ * own count); finished tests are retired into the result queue. */
+int lnt_batch_run(lnt_batch* b, uint64_t iterations);
+
+/* Move up to `cap` finished results to `out` (count in *count). */
+int lnt_batch_poll(lnt_batch* b, lnt_batch_result* out, int cap, int* count);
+
+/* Tests in flight and device bytes they hold. */
+int lnt_batch_status(lnt_batch* b, uint32_t* active, uint64_t* bytes_in_use);
+
 /* No counterpart in the reference.  For callers that cannot allocate device
  * memory when they need a residue in the reference's digit format (a serving
  * process whose HBM is all handed to its own pool or budget, a latency-critical
