@@ -50,6 +50,12 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--iterations-per-step", type=int, default=ITERATIONS_PER_STEP)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["c2", "c3", "c4", "c5"], default="c2",
+                    help="c2: one 8M-point LL test (default); c3/c4: batched tests/hour; c5: serving")
+    ap.add_argument("--seconds", type=float, default=30.0, help="timed window of c3/c4/c5")
+    ap.add_argument("--rates", default="0.5,1,2", help="c5: arrival rates as multiples of plain capacity")
+    ap.add_argument("--c5-range", default="10000,200000",
+                    help="c5: exponent range (full tests must finish inside the timed window)")
     return ap.parse_args()
 
 
@@ -170,11 +176,154 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- batches ----
+
+def primes_between(lo: int, hi: int) -> list[int]:
+    import numpy as np
+
+    sieve = np.ones(hi + 1, dtype=bool)
+    sieve[:2] = False
+    for k in range(2, int(hi ** 0.5) + 1):
+        if sieve[k]:
+            sieve[k * k::k] = False
+    return [int(x) for x in np.nonzero(sieve)[0] if x >= lo]
+
+
+def plain_us_per_iteration(cuda_b200, exponent: int, prp: bool, iters: int = 200) -> float:
+    """One test alone through the single-test path (the reference's way)."""
+    import torch
+
+    with cuda_b200.LucasTest(exponent, 0, prp) as t:
+        t.iterate(20)
+        t.synchronize()
+        t0 = time.perf_counter()
+        t.iterate(iters)
+        t.synchronize()
+        return (time.perf_counter() - t0) * 1e6 / iters
+
+
+def run_batch_workload(args, exps, prp, target_of, label, config):
+    """tests/hour of the batch engine against one-test-at-a-time, on a bounded window."""
+    import cuda_b200
+
+    step = 50
+    with cuda_b200.Batch(device=0) as b:
+        ids = {}
+        for q in exps:
+            ids[b.submit(q, 0, prp, target_of(q))] = q
+        for _ in range(3):
+            b.run(step)
+        steps = 0
+        t0 = time.perf_counter()
+        while time.perf_counter() - t0 < args.seconds:
+            b.run(step)
+            steps += 1
+        elapsed = time.perf_counter() - t0
+        finished = b.poll()
+    done_fraction = sum(min(1.0, steps * step / target_of(q)) for q in exps)
+    tests_per_hour = done_fraction / elapsed * 3600
+    # plain path: a sample spread over the exponents, each test alone
+    sample = sorted(exps)[:: max(1, len(exps) // 12)]
+    times = [target_of(q) * plain_us_per_iteration(cuda_b200, q, prp) * 1e-6 for q in sample]
+    plain_tests_per_hour = 3600 / (sum(times) / len(times))
+    line = {"metric": f"tests/hour, {label}", "value": tests_per_hour, "unit": "tests/hour",
+            "higher_is_better": True, "n_gpus": 1, "data": "synthetic (seeded exponents)",
+            "dtype": "u64", "config": config,
+            "plain_tests_per_hour": plain_tests_per_hour, "speedup_vs_plain": tests_per_hour / plain_tests_per_hour,
+            "window_s": elapsed, "squarings_per_test_in_window": steps * step,
+            "plain_sample": len(sample), "finished_in_window": len(finished)}
+    print(json.dumps(line), flush=True)
+
+
+def run_serving(args):
+    """Poisson stream of LL/PRP requests against the continuous-batching engine,
+    beside the plain sequential path (a FIFO queue over measured service times)."""
+    import math
+    import random
+
+    import numpy as np
+
+    import cuda_b200
+
+    lo, hi = (int(x) for x in args.c5_range.split(","))
+    primes = primes_between(lo, min(hi * 2, hi + 100000))
+    rng = random.Random(2)
+
+    def draw():
+        x = math.exp(rng.uniform(math.log(lo), math.log(hi)))
+        import bisect
+        return primes[min(bisect.bisect_left(primes, int(x)), len(primes) - 1)], rng.random() < 0.5
+
+    pool = [draw() for _ in range(64)]
+    service = [(q if prp else q - 2) * plain_us_per_iteration(cuda_b200, q, prp, 100) * 1e-6
+               for q, prp in pool[:16]]
+    mean_service = sum(service) / len(service)
+    plain_capacity = 1.0 / mean_service  # tests per second, one at a time
+    budget = 150 << 30
+    for mult in (float(r) for r in args.rates.split(",")):
+        rate = mult * plain_capacity
+        t = 0.0
+        arrivals = []
+        while t < args.seconds:
+            t += rng.expovariate(rate)
+            q, prp = pool[rng.randrange(len(pool))]
+            arrivals.append((t, q, prp))
+        arrivals = [a for a in arrivals if a[0] < args.seconds]
+        lat, done = [], 0
+        with cuda_b200.Batch(device=0, hbm_budget_bytes=budget) as b:
+            t0 = time.perf_counter()
+            k, enq = 0, {}
+            while (k < len(arrivals) or done < len(arrivals)) and time.perf_counter() - t0 < 4 * args.seconds:
+                now = time.perf_counter() - t0
+                while k < len(arrivals) and arrivals[k][0] <= now:
+                    i = b.enqueue(arrivals[k][1], 0, arrivals[k][2])
+                    enq[i] = now - arrivals[k][0]  # wait before enqueue
+                    k += 1
+                b.run(200)
+                for r in b.poll():
+                    lat.append(r["seconds"] + enq.pop(r["id"], 0.0))
+                    done += 1
+            wall = time.perf_counter() - t0
+        # plain sequential path: FIFO over the same arrivals, service = measured per-test time
+        serv = {}
+        free_at, plain_lat = 0.0, []
+        for (ta, q, prp) in arrivals:
+            if (q, prp) not in serv:
+                serv[(q, prp)] = (q if prp else q - 2) * plain_us_per_iteration(cuda_b200, q, prp, 100) * 1e-6
+            start = max(free_at, ta)
+            free_at = start + serv[(q, prp)]
+            plain_lat.append(free_at - ta)
+        line = {"metric": "serving p50/p99 latency and tests/hour", "rate_multiple_of_plain_capacity": mult,
+                "requests": len(arrivals), "completed": done, "wall_s": wall,
+                "p50_s": float(np.percentile(lat, 50)) if lat else None,
+                "p99_s": float(np.percentile(lat, 99)) if lat else None,
+                "tests_per_hour": done / wall * 3600,
+                "plain_p50_s": float(np.percentile(plain_lat, 50)), "plain_p99_s": float(np.percentile(plain_lat, 99)),
+                "plain_tests_per_hour": len(arrivals) / free_at * 3600 if free_at else None,
+                "config": {"exponents": f"primes log-uniform in [{lo}, {hi}], LL/PRP by a seeded coin (seed 2)",
+                           "hbm_budget_gb": 150, "arrival": "Poisson"}}
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     rank, local_rank, world = rank_info()
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload in ("c3", "c4", "c5"):
+        import random
+
+        if args.workload == "c3":
+            exps = random.Random(0).sample(primes_between(100000, 2000000), 256)
+            run_batch_workload(args, exps, False, lambda q: q - 2, "256 full LL tests, q in [1e5, 2e6] (seed 0)",
+                               {"workload": "C3 batch", "count": 256, "lengths": "4K-128K"})
+        elif args.workload == "c4":
+            exps = random.Random(1).sample(primes_between(5000000, 20000000), 64)
+            run_batch_workload(args, exps, True, lambda q: 20000, "64 PRP tests x 20000 squarings, q in [5e6, 2e7] (seed 1)",
+                               {"workload": "C4 batch", "count": 64, "lengths": "512K-1M"})
+        else:
+            run_serving(args)
         return
 
     import torch

@@ -87,6 +87,8 @@ def lib() -> ctypes.CDLL:
         "lnt_batch_destroy": ([vp], i32),
         "lnt_batch_submit": ([vp, u32, u32, i32, u64, ctypes.POINTER(u64)], i32),
         "lnt_batch_run": ([vp, u64], i32),
+        "lnt_batch_enqueue": ([vp, u32, u32, i32, u64, ctypes.POINTER(u64)], i32),
+        "lnt_batch_pending": ([vp, ctypes.POINTER(u32)], i32),
         "lnt_batch_poll": ([vp, ctypes.POINTER(BatchResult), i32, ctypes.POINTER(i32)], i32),
         "lnt_batch_status": ([vp, ctypes.POINTER(u32), ctypes.POINTER(u64)], i32),
     }
@@ -259,6 +261,18 @@ class Batch:
             return None
         _check(st, "lnt_batch_submit")
         return int(i.value)
+
+    def enqueue(self, exponent: int, n: int = 0, prp: bool = False, iterations: int = 0) -> int:
+        """Queue a test; it is admitted when the budget allows.  Returns its id."""
+        i = ctypes.c_uint64()
+        _check(lib().lnt_batch_enqueue(self._h, exponent, n, int(bool(prp)), int(iterations),
+                                       ctypes.byref(i)), "lnt_batch_enqueue")
+        return int(i.value)
+
+    def pending(self) -> int:
+        c = ctypes.c_uint32()
+        _check(lib().lnt_batch_pending(self._h, ctypes.byref(c)), "lnt_batch_pending")
+        return int(c.value)
 
     def run(self, iterations: int) -> None:
         _check(lib().lnt_batch_run(self._h, int(iterations)), "lnt_batch_run")

@@ -35,6 +35,14 @@ struct Entry {
   Clock::time_point submitted;
 };
 
+struct Pending {
+  uint64_t id;
+  uint32_t q, n;
+  int prp;
+  uint64_t iterations;
+  Clock::time_point enqueued;
+};
+
 struct Group {
   uint32_t n = 0;
   std::vector<size_t> members;  // indices into active
@@ -57,6 +65,7 @@ struct lnt_batch {
   uint64_t next_id = 1;
   cudaStream_t stream = nullptr;
   std::vector<Entry> active;
+  std::deque<Pending> pending;  // enqueued, waiting for budget
   std::deque<lnt_batch_result> finished;
   // launch groups, rebuilt when membership changes
   bool dirty = true;
@@ -214,20 +223,19 @@ int lnt_batch_destroy(lnt_batch* b) {
   return LNT_OK;
 }
 
-int lnt_batch_submit(lnt_batch* b, uint32_t exponent, uint32_t n, int prp, uint64_t iterations,
-                     uint64_t* id) {
-  if (!b) return berr(LNT_ERR_INVALID_ARGUMENT, "null batch");
-  DeviceGuard guard(b->device);
-  if (n == 0) n = 1u << lnt_secured_log2_length(exponent);
+}  // extern "C"
+
+namespace {
+
+// Create the test's state on the device and add it to the active set.
+int admit(lnt_batch* b, uint64_t id, uint32_t exponent, uint32_t n, int prp, uint64_t iterations,
+          Clock::time_point since) {
   const uint64_t bytes = lnt::test_device_bytes(n);
-  if (bytes == 0) return berr(LNT_ERR_UNSUPPORTED_LENGTH, "unsupported length");
-  if (b->budget && b->used + bytes > b->budget)
-    return berr(LNT_ERR_BUDGET, "test does not fit the HBM budget");
   lnt_test* t = nullptr;
   int st = lnt_create(exponent, n, prp, b->device, &t);
   if (st != LNT_OK) return st;
   Entry e{};
-  e.id = b->next_id++;
+  e.id = id;
   e.t = t;
   e.q = exponent;
   e.n = n;
@@ -235,7 +243,7 @@ int lnt_batch_submit(lnt_batch* b, uint32_t exponent, uint32_t n, int prp, uint6
   e.target = iterations ? iterations : (prp ? (uint64_t)exponent : (uint64_t)exponent - 2);
   e.done = 0;
   e.bytes = bytes;
-  e.submitted = Clock::now();
+  e.submitted = since;
   const lnt::Plan& p = lnt::test_plan(t);
   if (p.kind == lnt::PlanKind::TwoPass && e.target > 0) {
     // the first squaring reads non-negative digits (unsigned outputs): run it
@@ -249,15 +257,68 @@ int lnt_batch_submit(lnt_batch* b, uint32_t exponent, uint32_t n, int prp, uint6
   b->used += bytes;
   b->active.push_back(e);
   b->dirty = true;
-  if (id) *id = e.id;
+  return LNT_OK;
+}
+
+// Admit queued tests first-fit while the budget allows.
+int admit_pending(lnt_batch* b) {
+  for (auto it = b->pending.begin(); it != b->pending.end();) {
+    const uint64_t bytes = lnt::test_device_bytes(it->n);
+    if (b->budget && b->used + bytes > b->budget) {
+      ++it;
+      continue;
+    }
+    const int st = admit(b, it->id, it->q, it->n, it->prp, it->iterations, it->enqueued);
+    if (st != LNT_OK) return st;
+    it = b->pending.erase(it);
+  }
+  return LNT_OK;
+}
+
+int check_request(uint32_t exponent, uint32_t& n) {
+  if (n == 0) n = 1u << lnt_secured_log2_length(exponent);
+  if (lnt::test_device_bytes(n) == 0) return berr(LNT_ERR_UNSUPPORTED_LENGTH, "unsupported length");
+  return LNT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lnt_batch_submit(lnt_batch* b, uint32_t exponent, uint32_t n, int prp, uint64_t iterations,
+                     uint64_t* id) {
+  if (!b) return berr(LNT_ERR_INVALID_ARGUMENT, "null batch");
+  DeviceGuard guard(b->device);
+  int st = check_request(exponent, n);
+  if (st != LNT_OK) return st;
+  if (b->budget && b->used + lnt::test_device_bytes(n) > b->budget)
+    return berr(LNT_ERR_BUDGET, "test does not fit the HBM budget");
+  const uint64_t new_id = b->next_id++;
+  if ((st = admit(b, new_id, exponent, n, prp, iterations, Clock::now())) != LNT_OK) return st;
+  if (id) *id = new_id;
   return retire_finished(b);
+}
+
+int lnt_batch_enqueue(lnt_batch* b, uint32_t exponent, uint32_t n, int prp, uint64_t iterations,
+                      uint64_t* id) {
+  if (!b) return berr(LNT_ERR_INVALID_ARGUMENT, "null batch");
+  DeviceGuard guard(b->device);
+  int st = check_request(exponent, n);
+  if (st != LNT_OK) return st;
+  if (b->budget && lnt::test_device_bytes(n) > b->budget)
+    return berr(LNT_ERR_BUDGET, "test larger than the whole HBM budget");
+  Pending p{b->next_id++, exponent, n, prp ? 1 : 0, iterations, Clock::now()};
+  b->pending.push_back(p);
+  if (id) *id = p.id;
+  return admit_pending(b);
 }
 
 int lnt_batch_run(lnt_batch* b, uint64_t iterations) {
   if (!b) return berr(LNT_ERR_INVALID_ARGUMENT, "null batch");
   DeviceGuard guard(b->device);
+  int st = admit_pending(b);
+  if (st != LNT_OK) return st;
   if (b->active.empty() || iterations == 0) return LNT_OK;
-  int st;
   if (b->dirty && (st = rebuild(b)) != LNT_OK) return st;
   // grouped tests advance in lockstep: no test of a group may pass its target
   uint64_t k = iterations;
@@ -306,7 +367,8 @@ int lnt_batch_run(lnt_batch* b, uint64_t iterations) {
     Entry& e = b->active[i];
     e.done += std::min(iterations, e.target - e.done);
   }
-  return retire_finished(b);
+  if ((st = retire_finished(b)) != LNT_OK) return st;
+  return admit_pending(b);
 }
 
 int lnt_batch_poll(lnt_batch* b, lnt_batch_result* out, int cap, int* count) {
@@ -324,6 +386,12 @@ int lnt_batch_status(lnt_batch* b, uint32_t* active, uint64_t* bytes_in_use) {
   if (!b) return berr(LNT_ERR_INVALID_ARGUMENT, "null batch");
   if (active) *active = (uint32_t)b->active.size();
   if (bytes_in_use) *bytes_in_use = b->used;
+  return LNT_OK;
+}
+
+int lnt_batch_pending(lnt_batch* b, uint32_t* pending) {
+  if (!b || !pending) return berr(LNT_ERR_INVALID_ARGUMENT, "null argument");
+  *pending = (uint32_t)b->pending.size();
   return LNT_OK;
 }
 

@@ -167,15 +167,24 @@ int lnt_batch_destroy(lnt_batch* b);
 int lnt_batch_submit(lnt_batch* b, uint32_t exponent, uint32_t n, int prp, uint64_t iterations,
                      uint64_t* id);
 
+/* Like lnt_batch_submit, but a test that does not fit the budget now waits in
+ * a queue and is admitted (first fit) as soon as retired tests free memory;
+ * its result's `seconds` count from this call.  LNT_ERR_BUDGET only for a
+ * test larger than the whole budget. */
+int lnt_batch_enqueue(lnt_batch* b, uint32_t exponent, uint32_t n, int prp, uint64_t iterations,
+                      uint64_t* id);
+
 /* Advance every admitted test by up to `iterations` squarings (none passes its
- * own count); finished tests are retired into the result queue. */
+ * own count); finished tests are retired into the result queue and queued
+ * tests admitted. */
 int lnt_batch_run(lnt_batch* b, uint64_t iterations);
 
 /* Move up to `cap` finished results to `out` (count in *count). */
 int lnt_batch_poll(lnt_batch* b, lnt_batch_result* out, int cap, int* count);
 
-/* Tests in flight and device bytes they hold. */
+/* Tests in flight and device bytes they hold; tests waiting in the queue. */
 int lnt_batch_status(lnt_batch* b, uint32_t* active, uint64_t* bytes_in_use);
+int lnt_batch_pending(lnt_batch* b, uint32_t* pending);
 
 /* No counterpart in the reference.  For callers that cannot allocate device
  * memory when they need a residue in the reference's digit format (a serving
