@@ -7,10 +7,14 @@ from .api import (  # noqa: F401
     Batch,
     LucasNTTError,
     LucasTest,
+    PlanOptions,
+    autotune,
     check_provided_length,
     length_candidates,
     lib,
     parse_length,
+    plan_candidates,
+    plan_describe,
     secured_log2_length,
     test_device_bytes,
 )

@@ -41,6 +41,14 @@ class BatchResult(ctypes.Structure):
                 ("prp", ctypes.c_int), ("is_prime", ctypes.c_int), ("status", ctypes.c_int)]
 
 
+class PlanOptions(ctypes.Structure):
+    """lnt_plan_options: kernel family (1 resident, 2 radix-16, 3 radix-2), log2 n2, tile."""
+    _fields_ = [("kind", ctypes.c_uint32), ("log2_rows", ctypes.c_uint32), ("tile", ctypes.c_uint32)]
+
+    def as_tuple(self) -> tuple[int, int, int]:
+        return int(self.kind), int(self.log2_rows), int(self.tile)
+
+
 class LucasNTTError(RuntimeError):
     def __init__(self, status: int, where: str):
         L = lib()
@@ -68,6 +76,12 @@ def lib() -> ctypes.CDLL:
         "lnt_parse_length": ([cp, ctypes.POINTER(u32)], i32),
         "lnt_check_provided_length": ([u32, cp, ctypes.POINTER(i32)], i32),
         "lnt_create": ([u32, u32, i32, i32, ctypes.POINTER(vp)], i32),
+        "lnt_create_with_plan": ([u32, u32, i32, i32, ctypes.POINTER(PlanOptions), ctypes.POINTER(vp)], i32),
+        "lnt_get_plan": ([vp, ctypes.POINTER(PlanOptions)], i32),
+        "lnt_plan_candidates": ([u32, u32, ctypes.POINTER(PlanOptions), i32, ctypes.POINTER(i32)], i32),
+        "lnt_plan_describe": ([ctypes.POINTER(PlanOptions), u32, u32, cp, sz], i32),
+        "lnt_autotune": ([u32, u32, i32, i32, u32, ctypes.POINTER(PlanOptions), ctypes.POINTER(ctypes.c_float),
+                          i32, ctypes.POINTER(i32), ctypes.POINTER(i32)], i32),
         "lnt_destroy": ([vp], i32),
         "lnt_init_test": ([vp], i32),
         "lnt_iterate": ([vp, u64], i32),
@@ -91,6 +105,8 @@ def lib() -> ctypes.CDLL:
         "lnt_batch_pending": ([vp, ctypes.POINTER(u32)], i32),
         "lnt_batch_poll": ([vp, ctypes.POINTER(BatchResult), i32, ctypes.POINTER(i32)], i32),
         "lnt_batch_status": ([vp, ctypes.POINTER(u32), ctypes.POINTER(u64)], i32),
+        "lnt_batch_autotune": ([vp, u32], i32),
+        "lnt_batch_use_graphs": ([vp, i32], i32),
     }
     for name, (args, res) in sigs.items():
         f = getattr(L, name)
@@ -132,12 +148,43 @@ def check_provided_length(exponent: int, description: str) -> int:
     return int(d.value)
 
 
+def plan_candidates(exponent: int, n: int = 0) -> list[tuple[int, int, int]]:
+    """Every valid plan (kind, log2 n2, tile) for (q, n): lnt_plan_candidates."""
+    buf = (PlanOptions * 64)()
+    c = ctypes.c_int()
+    _check(lib().lnt_plan_candidates(exponent, n, buf, 64, ctypes.byref(c)), "lnt_plan_candidates")
+    return [buf[i].as_tuple() for i in range(min(c.value, 64))]
+
+
+def plan_describe(plan: tuple[int, int, int], exponent: int, n: int = 0) -> str:
+    buf = ctypes.create_string_buffer(128)
+    o = PlanOptions(*plan)
+    _check(lib().lnt_plan_describe(ctypes.byref(o), exponent, n, buf, 128), "lnt_plan_describe")
+    return buf.value.decode()
+
+
+def autotune(exponent: int, n: int = 0, prp: bool = False, device: int = 0, loops: int = 100):
+    """lnt_autotune: [(plan, ms for `loops` squarings or -1)], index of the fastest."""
+    tried = (PlanOptions * 64)()
+    ms = (ctypes.c_float * 64)()
+    c, b = ctypes.c_int(), ctypes.c_int()
+    _check(lib().lnt_autotune(exponent, n, int(bool(prp)), device, loops, tried, ms, 64, ctypes.byref(c),
+                              ctypes.byref(b)), "lnt_autotune")
+    return [(tried[i].as_tuple(), float(ms[i])) for i in range(min(c.value, 64))], int(b.value)
+
+
 class LucasTest:
     """One Lucas-Lehmer (prp=False) or base-3 PRP test of M = 2^exponent - 1."""
 
-    def __init__(self, exponent: int, n: int = 0, prp: bool = False, device: int = 0):
+    def __init__(self, exponent: int, n: int = 0, prp: bool = False, device: int = 0,
+                 plan: tuple[int, int, int] | None = None):
         h = ctypes.c_void_p()
-        _check(lib().lnt_create(exponent, n, int(bool(prp)), device, ctypes.byref(h)), "lnt_create")
+        if plan is None:
+            _check(lib().lnt_create(exponent, n, int(bool(prp)), device, ctypes.byref(h)), "lnt_create")
+        else:
+            o = PlanOptions(*plan)
+            _check(lib().lnt_create_with_plan(exponent, n, int(bool(prp)), device, ctypes.byref(o),
+                                              ctypes.byref(h)), "lnt_create_with_plan")
         self._h = h
         self.exponent = int(exponent)
         self.prp = bool(prp)
@@ -205,6 +252,11 @@ class LucasTest:
         _check(lib().lnt_plan_name(self._h, buf, 64), "lnt_plan_name")
         return buf.value.decode()
 
+    def plan_options(self) -> tuple[int, int, int]:
+        o = PlanOptions()
+        _check(lib().lnt_get_plan(self._h, ctypes.byref(o)), "lnt_get_plan")
+        return o.as_tuple()
+
     def set_stream(self, stream_handle: int | None) -> None:
         _check(lib().lnt_set_stream(self._h, stream_handle), "lnt_set_stream")
 
@@ -231,10 +283,15 @@ class Batch:
     """Many LL / PRP tests on one GPU, admitted under an HBM budget and retired
     as they finish (lnt_batch_*)."""
 
-    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0):
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, autotune_loops: int = 0,
+                 graphs: bool = True):
         h = ctypes.c_void_p()
         _check(lib().lnt_batch_create(device, int(hbm_budget_bytes), ctypes.byref(h)), "lnt_batch_create")
         self._h = h
+        if autotune_loops:
+            _check(lib().lnt_batch_autotune(self._h, int(autotune_loops)), "lnt_batch_autotune")
+        if not graphs:
+            _check(lib().lnt_batch_use_graphs(self._h, 0), "lnt_batch_use_graphs")
 
     def close(self) -> None:
         if getattr(self, "_h", None):

@@ -419,13 +419,14 @@ void test_mark_iterated(lnt_test* t) {
 // Device bytes lnt_create allocates for a test (the batch engine's budget unit).
 uint64_t test_device_bytes(uint32_t n) {
   Plan plan;
-  if (!make_plan(n, plan)) return 0;
+  if (!make_plan(n, 0, nullptr, plan)) return 0;
   const uint64_t nb = n / canon_block_size(n);
   uint64_t b = 8ull * n * 4 + n + 4 + nb * 10 + 4;  // x, w, uw, canon, widths, status, readout
   if (plan.kind == PlanKind::Resident) {
     b += 8ull * n + sizeof(ResidentDesc);  // root tables
   } else {
-    b += 16ull * n + 8ull * (plan.n1 + plan.n2) + 8ull * plan.ntiles * plan.n2 + sizeof(TwoPassDesc);
+    // carry buffer: one word per run, at most n / 4 runs (the narrowest tile)
+    b += 16ull * n + 8ull * (plan.n1 + plan.n2) + 2ull * n + sizeof(TwoPassDesc);
     if (plan.fast) b += 16ull * (plan.n1 + plan.n2) + 17ull * n;  // inner twiddles, tile-major tables
   }
   return b;
@@ -451,6 +452,11 @@ const char* lnt_status_string(int status) {
 const char* lnt_last_error(void) { return g_last_error.c_str(); }
 
 int lnt_create(uint32_t exponent, uint32_t n, int prp, int device, lnt_test** out) {
+  return lnt_create_with_plan(exponent, n, prp, device, nullptr, out);
+}
+
+int lnt_create_with_plan(uint32_t exponent, uint32_t n, int prp, int device,
+                         const lnt_plan_options* options, lnt_test** out) {
   if (!out) return fail(LNT_ERR_INVALID_ARGUMENT, "null output pointer");
   *out = nullptr;
   if (exponent < 3) return fail(LNT_ERR_INVALID_ARGUMENT, "exponent must be >= 3");
@@ -460,12 +466,14 @@ int lnt_create(uint32_t exponent, uint32_t n, int prp, int device, lnt_test** ou
     n = 1u << l;
   }
   lnt::Plan plan;
-  if (!lnt::make_plan(n, plan)) return fail(LNT_ERR_UNSUPPORTED_LENGTH, "length must be 2^k, 1 <= k <= 26");
-  if (plan.fast && plan.tile == 8 && lnt::r16_run_words_needed(exponent, plan.log2n) <= 4) {
-    // carry runs of 4 words suffice: narrower column tiles, two CTAs per SM
-    plan.tile = 4;
-    plan.ntiles = plan.n1 / plan.tile;
+  lnt::PlanOptions opt;
+  if (options) {
+    opt.kind = options->kind;
+    opt.log2_rows = options->log2_rows;
+    opt.tile = options->tile;
   }
+  std::string why;
+  if (!lnt::make_plan(n, exponent, &opt, plan, &why)) return fail(LNT_ERR_UNSUPPORTED_LENGTH, why);
   if (n > exponent) return fail(LNT_ERR_UNSUPPORTED_LENGTH, "length exceeds the exponent");
   if ((exponent + n - 1) / n > 30) return fail(LNT_ERR_UNSUPPORTED_LENGTH, "more than 30 bits per word");
   int count = 0;
@@ -664,6 +672,91 @@ int lnt_get_widths(lnt_test* t, uint8_t* widths, size_t n) {
   if (!t || !widths || n != t->n) return fail(LNT_ERR_INVALID_ARGUMENT, "widths/length mismatch");
   std::memcpy(widths, t->h_widths.data(), n);
   return LNT_OK;
+}
+
+int lnt_get_plan(lnt_test* t, lnt_plan_options* out) {
+  if (!t || !out) return fail(LNT_ERR_INVALID_ARGUMENT, "null argument");
+  const lnt::Plan& p = t->plan;
+  out->kind = p.kind == lnt::PlanKind::Resident ? LNT_PLAN_RESIDENT
+                                                : (p.fast ? LNT_PLAN_RADIX16 : LNT_PLAN_RADIX2);
+  out->log2_rows = p.kind == lnt::PlanKind::Resident ? 0 : p.log2n2;
+  out->tile = p.kind == lnt::PlanKind::Resident ? 0 : p.tile;
+  return LNT_OK;
+}
+
+int lnt_plan_candidates(uint32_t exponent, uint32_t n, lnt_plan_options* out, int cap, int* count) {
+  if (!count || (cap > 0 && !out)) return fail(LNT_ERR_INVALID_ARGUMENT, "null argument");
+  if (n == 0) n = 1u << lnt_secured_log2_length(exponent);
+  const std::vector<lnt::PlanOptions> c = lnt::plan_candidates(n, exponent);
+  *count = (int)c.size();
+  for (int i = 0; i < cap && i < (int)c.size(); ++i) out[i] = {c[i].kind, c[i].log2_rows, c[i].tile};
+  return c.empty() ? fail(LNT_ERR_UNSUPPORTED_LENGTH, "no plan for this length") : LNT_OK;
+}
+
+int lnt_plan_describe(const lnt_plan_options* o, uint32_t exponent, uint32_t n, char* out,
+                      size_t outlen) {
+  if (!o || !out || outlen == 0) return fail(LNT_ERR_INVALID_ARGUMENT, "null argument");
+  if (n == 0) n = 1u << lnt_secured_log2_length(exponent);
+  lnt::Plan plan;
+  lnt::PlanOptions opt;
+  opt.kind = o->kind;
+  opt.log2_rows = o->log2_rows;
+  opt.tile = o->tile;
+  std::string why;
+  if (!lnt::make_plan(n, exponent, &opt, plan, &why)) return fail(LNT_ERR_UNSUPPORTED_LENGTH, why);
+  std::snprintf(out, outlen, "%s", plan.name.c_str());
+  return LNT_OK;
+}
+
+// Process::GetBestPerformers (process.cu:45-127) over this library's plans:
+// every candidate runs `loops` squarings after a short warm-up, timed with CUDA
+// events on its stream; the fastest wins.
+int lnt_autotune(uint32_t exponent, uint32_t n, int prp, int device, uint32_t loops,
+                 lnt_plan_options* tried, float* ms, int cap, int* count, int* best) {
+  if (!count || !best || (cap > 0 && (!tried || !ms))) return fail(LNT_ERR_INVALID_ARGUMENT, "null argument");
+  if (loops == 0) return fail(LNT_ERR_INVALID_ARGUMENT, "loops must be > 0");
+  if (n == 0) n = 1u << lnt_secured_log2_length(exponent);
+  const std::vector<lnt::PlanOptions> c = lnt::plan_candidates(n, exponent);
+  *count = 0;
+  *best = -1;
+  float best_ms = 0;
+  int last_status = LNT_ERR_UNSUPPORTED_LENGTH;
+  for (size_t i = 0; i < c.size(); ++i) {
+    const lnt_plan_options o = {c[i].kind, c[i].log2_rows, c[i].tile};
+    lnt_test* t = nullptr;
+    float elapsed = -1;
+    int st = lnt_create_with_plan(exponent, n, prp, device, &o, &t);
+    if (st == LNT_OK) {
+      DeviceGuard guard(t->device);
+      cudaEvent_t e0 = nullptr, e1 = nullptr;
+      const uint64_t warm = loops / 10 + 2;
+      if ((st = lnt_iterate(t, warm)) == LNT_OK && (st = lnt_synchronize(t)) == LNT_OK) {
+        if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess ||
+            cudaEventRecord(e0, t->stream) != cudaSuccess)
+          st = fail(LNT_ERR_CUDA, "autotune events");
+        else if ((st = lnt_iterate(t, loops)) == LNT_OK &&
+                 cudaEventRecord(e1, t->stream) == cudaSuccess &&
+                 cudaEventSynchronize(e1) == cudaSuccess &&
+                 (st = lnt_synchronize(t)) == LNT_OK)
+          cudaEventElapsedTime(&elapsed, e0, e1);
+      }
+      if (e0) cudaEventDestroy(e0);
+      if (e1) cudaEventDestroy(e1);
+      lnt_destroy(t);
+    }
+    if (st == LNT_ERR_NO_DEVICE || st == LNT_ERR_CUDA) return st;
+    last_status = st;
+    if ((int)i < cap) {
+      tried[i] = o;
+      ms[i] = st == LNT_OK ? elapsed : -1.0f;
+    }
+    ++*count;
+    if (st == LNT_OK && elapsed >= 0 && (*best < 0 || elapsed < best_ms)) {
+      *best = (int)i;
+      best_ms = elapsed;
+    }
+  }
+  return *best >= 0 ? LNT_OK : last_status;
 }
 
 int lnt_plan_name(lnt_test* t, char* out, size_t outlen) {

@@ -10,6 +10,13 @@
 // their own streams so small groups overlap.  Tests are admitted against an
 // HBM budget and retired (Res64 and verdict recorded, memory released) as they
 // finish, so a caller can keep the engine full: continuous batching.
+//
+// The grouped launches of `kGraphChunk` squarings are captured once per group
+// membership into a CUDA graph (fork/join over the group streams) and replayed,
+// so a batch step costs one graph launch per chunk instead of 3 x groups x
+// chunk kernel launches.  Optionally (lnt_batch_autotune) each length's plan
+// (split, column tile) is picked by timing the candidates once per length,
+// the analogue of the reference's per-run autotune (process.cu:45-127).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -43,6 +50,18 @@ struct Pending {
   Clock::time_point enqueued;
 };
 
+// Tests share launches when their kernels see the same geometry.
+struct GroupKey {
+  uint32_t n, log2n2, tile;
+  bool operator<(const GroupKey& o) const {
+    if (n != o.n) return n < o.n;
+    if (log2n2 != o.log2n2) return log2n2 < o.log2n2;
+    return tile < o.tile;
+  }
+};
+
+constexpr uint64_t kGraphChunk = 8;  // squarings per captured graph
+
 struct Group {
   uint32_t n = 0;
   std::vector<size_t> members;  // indices into active
@@ -50,6 +69,7 @@ struct Group {
   lnt::TwoPassDesc* d_descs = nullptr;
   size_t cap = 0;
   cudaStream_t stream = nullptr;
+  cudaEvent_t join = nullptr;  // recorded on `stream` after the group's launches
 };
 
 int berr(int status, const std::string& msg) {
@@ -69,12 +89,20 @@ struct lnt_batch {
   std::deque<lnt_batch_result> finished;
   // launch groups, rebuilt when membership changes
   bool dirty = true;
-  std::map<uint64_t, Group> groups;  // fast two-pass tests by (length, tile width)
+  std::map<GroupKey, Group> groups;  // fast two-pass tests by geometry
   std::vector<size_t> resident;      // SMEM-resident tests
   std::vector<size_t> singles;       // tests iterated one by one
   lnt::ResidentDesc* d_rdescs = nullptr;
   size_t rcap = 0;
   std::vector<cudaStream_t> spare_streams;
+  cudaStream_t rstream = nullptr;    // the resident launch, beside the groups
+  cudaEvent_t fork = nullptr;        // recorded on `stream` before the group launches
+  // graph of kGraphChunk squarings of every group, valid until membership changes
+  cudaGraphExec_t graph = nullptr;
+  bool use_graphs = true;
+  // autotuned plans: (n, shortest valid run) -> plan; loops = 0: policy plans
+  uint32_t tune_loops = 0;
+  std::map<uint64_t, lnt_plan_options> tuned;
 };
 
 namespace {
@@ -109,9 +137,55 @@ cudaStream_t take_stream(lnt_batch* b) {
   return s;
 }
 
+void drop_graph(lnt_batch* b) {
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  b->graph = nullptr;
+}
+
+// One chunk of squarings of every group, forked from b->stream onto the group
+// streams and joined back (the body of the captured graph).
+int launch_groups(lnt_batch* b, uint64_t k) {
+  BCUDA(cudaEventRecord(b->fork, b->stream), "fork");
+  for (auto& kv : b->groups) {
+    Group& g = kv.second;
+    const uint32_t cnt = (uint32_t)g.members.size();
+    BCUDA(cudaStreamWaitEvent(g.stream, b->fork, 0), "fork wait");
+    for (uint64_t it = 0; it < k; ++it) {
+      BCUDA(lnt::launch_col_forward_r16(g.geometry, g.d_descs, cnt, true, g.stream), "col_forward");
+      BCUDA(lnt::launch_row_square_r16(g.geometry, g.d_descs, cnt, g.stream), "row_square");
+      BCUDA(lnt::launch_col_inverse_r16(g.geometry, g.d_descs, cnt, false, g.stream), "col_inverse");
+    }
+    BCUDA(cudaEventRecord(g.join, g.stream), "join");
+    BCUDA(cudaStreamWaitEvent(b->stream, g.join, 0), "join wait");
+  }
+  return LNT_OK;
+}
+
+int build_graph(lnt_batch* b) {
+  drop_graph(b);
+  BCUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+  const int st = launch_groups(b, kGraphChunk);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+  if (st != LNT_OK) {
+    if (g) cudaGraphDestroy(g);
+    return st;
+  }
+  if (e != cudaSuccess) return berr(LNT_ERR_CUDA, std::string("end capture: ") + cudaGetErrorString(e));
+  const cudaError_t ie = cudaGraphInstantiate(&b->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (ie != cudaSuccess) {
+    b->graph = nullptr;
+    return berr(LNT_ERR_CUDA, std::string("instantiate graph: ") + cudaGetErrorString(ie));
+  }
+  return LNT_OK;
+}
+
 int rebuild(lnt_batch* b) {
+  drop_graph(b);
   for (auto& kv : b->groups) {
     if (kv.second.d_descs) cudaFree(kv.second.d_descs);
+    if (kv.second.join) cudaEventDestroy(kv.second.join);
     b->spare_streams.push_back(kv.second.stream);
   }
   b->groups.clear();
@@ -123,7 +197,7 @@ int rebuild(lnt_batch* b) {
       b->resident.push_back(i);
     } else if (p.fast && lnt::test_ready_for_group(b->active[i].t)) {
       // one launch serves tests of identical geometry: same length and tile width
-      Group& g = b->groups[((uint64_t)p.n << 8) | p.tile];
+      Group& g = b->groups[GroupKey{p.n, p.log2n2, p.tile}];
       g.n = p.n;
       g.members.push_back(i);
     } else {
@@ -140,6 +214,7 @@ int rebuild(lnt_batch* b) {
     BCUDA(cudaMemcpy(g.d_descs, h.data(), h.size() * sizeof(lnt::TwoPassDesc), cudaMemcpyHostToDevice),
           "upload descriptors");
     g.stream = take_stream(b);
+    BCUDA(cudaEventCreateWithFlags(&g.join, cudaEventDisableTiming), "group event");
   }
   if (b->resident.size() > b->rcap) {
     if (b->d_rdescs) cudaFree(b->d_rdescs);
@@ -198,7 +273,11 @@ int lnt_batch_create(int device, uint64_t hbm_budget_bytes, lnt_batch** out) {
   lnt_batch* b = new lnt_batch();
   b->device = device;
   b->budget = hbm_budget_bytes;
-  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&b->rstream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess) {
+    if (b->stream) cudaStreamDestroy(b->stream);
+    if (b->rstream) cudaStreamDestroy(b->rstream);
     delete b;
     return berr(LNT_ERR_CUDA, "cudaStreamCreate");
   }
@@ -210,15 +289,19 @@ int lnt_batch_destroy(lnt_batch* b) {
   if (!b) return LNT_OK;
   DeviceGuard guard(b->device);
   cudaDeviceSynchronize();
+  drop_graph(b);
   for (auto& e : b->active) lnt_destroy(e.t);
   for (auto& kv : b->groups) {
     if (kv.second.d_descs) cudaFree(kv.second.d_descs);
+    if (kv.second.join) cudaEventDestroy(kv.second.join);
     if (kv.second.stream) cudaStreamDestroy(kv.second.stream);
   }
+  if (b->fork) cudaEventDestroy(b->fork);
   for (cudaStream_t s : b->spare_streams)
     if (s) cudaStreamDestroy(s);
   if (b->d_rdescs) cudaFree(b->d_rdescs);
   if (b->stream) cudaStreamDestroy(b->stream);
+  if (b->rstream) cudaStreamDestroy(b->rstream);
   delete b;
   return LNT_OK;
 }
@@ -232,7 +315,25 @@ int admit(lnt_batch* b, uint64_t id, uint32_t exponent, uint32_t n, int prp, uin
           Clock::time_point since) {
   const uint64_t bytes = lnt::test_device_bytes(n);
   lnt_test* t = nullptr;
-  int st = lnt_create(exponent, n, prp, b->device, &t);
+  const lnt_plan_options* plan = nullptr;
+  int st;
+  if (b->tune_loops && n > 4096) {
+    // one timing per (length, shortest carry run the exponent allows)
+    const uint32_t run = lnt::r16_run_words_needed(exponent, 31 - __builtin_clz(n)) <= 4 ? 4 : 8;
+    const uint64_t key = ((uint64_t)n << 8) | run;
+    auto it = b->tuned.find(key);
+    if (it == b->tuned.end()) {
+      lnt_plan_options tried[64];
+      float ms[64];
+      int count = 0, best = -1;
+      st = lnt_autotune(exponent, n, prp, b->device, b->tune_loops, tried, ms, 64, &count, &best);
+      lnt_plan_options chosen{};
+      if (st == LNT_OK && best >= 0 && best < 64) chosen = tried[best];
+      it = b->tuned.emplace(key, chosen).first;
+    }
+    plan = &it->second;
+  }
+  st = lnt_create_with_plan(exponent, n, prp, b->device, plan, &t);
   if (st != LNT_OK) return st;
   Entry e{};
   e.id = id;
@@ -324,7 +425,7 @@ int lnt_batch_run(lnt_batch* b, uint64_t iterations) {
   uint64_t k = iterations;
   for (auto& kv : b->groups)
     for (size_t i : kv.second.members) k = std::min(k, b->active[i].target - b->active[i].done);
-  // SMEM-resident tests: one launch, per-test counts
+  // SMEM-resident tests: one launch, per-test counts, beside the groups
   if (!b->resident.empty()) {
     std::vector<lnt::ResidentDesc> h;
     uint32_t max_n = 0;
@@ -334,18 +435,18 @@ int lnt_batch_run(lnt_batch* b, uint64_t iterations) {
       max_n = std::max(max_n, e.n);
     }
     BCUDA(cudaMemcpyAsync(b->d_rdescs, h.data(), h.size() * sizeof(lnt::ResidentDesc),
-                          cudaMemcpyHostToDevice, b->stream),
+                          cudaMemcpyHostToDevice, b->rstream),
           "upload resident descriptors");
-    BCUDA(lnt::launch_resident(b->d_rdescs, (uint32_t)h.size(), max_n, b->stream), "resident kernel");
+    BCUDA(lnt::launch_resident(b->d_rdescs, (uint32_t)h.size(), max_n, b->rstream), "resident kernel");
   }
-  for (auto& kv : b->groups) {
-    Group& g = kv.second;
-    const uint32_t cnt = (uint32_t)g.members.size();
-    for (uint64_t it = 0; it < k; ++it) {
-      BCUDA(lnt::launch_col_forward_r16(g.geometry, g.d_descs, cnt, true, g.stream), "col_forward");
-      BCUDA(lnt::launch_row_square_r16(g.geometry, g.d_descs, cnt, g.stream), "row_square");
-      BCUDA(lnt::launch_col_inverse_r16(g.geometry, g.d_descs, cnt, false, g.stream), "col_inverse");
+  if (!b->groups.empty() && k > 0) {
+    uint64_t left = k;
+    if (b->use_graphs && k >= kGraphChunk) {
+      if (!b->graph && (st = build_graph(b)) != LNT_OK) return st;
+      for (; left >= kGraphChunk; left -= kGraphChunk)
+        BCUDA(cudaGraphLaunch(b->graph, b->stream), "graph launch");
     }
+    if (left && (st = launch_groups(b, left)) != LNT_OK) return st;
   }
   for (size_t i : b->singles) {
     Entry& e = b->active[i];
@@ -369,6 +470,20 @@ int lnt_batch_run(lnt_batch* b, uint64_t iterations) {
   }
   if ((st = retire_finished(b)) != LNT_OK) return st;
   return admit_pending(b);
+}
+
+int lnt_batch_autotune(lnt_batch* b, uint32_t loops) {
+  if (!b) return berr(LNT_ERR_INVALID_ARGUMENT, "null batch");
+  b->tune_loops = loops;
+  return LNT_OK;
+}
+
+int lnt_batch_use_graphs(lnt_batch* b, int enable) {
+  if (!b) return berr(LNT_ERR_INVALID_ARGUMENT, "null batch");
+  DeviceGuard guard(b->device);
+  b->use_graphs = enable != 0;
+  if (!b->use_graphs) drop_graph(b);
+  return LNT_OK;
 }
 
 int lnt_batch_poll(lnt_batch* b, lnt_batch_result* out, int cap, int* count) {

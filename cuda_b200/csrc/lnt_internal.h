@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string>
+#include <vector>
 
 namespace lnt {
 
@@ -35,7 +36,20 @@ struct Plan {
 constexpr uint32_t kResidentMaxLog2 = 12;
 constexpr uint32_t kMaxLog2 = 26;  // (p - 1) / 192 holds 2^26: the largest IBDWT length
 
-bool make_plan(uint32_t n, Plan& plan);
+// Explicit choices for make_plan (the C ABI's lnt_plan_options); 0 = policy.
+struct PlanOptions {
+  uint32_t kind = 0;       // 0 policy, 1 resident, 2 two-pass radix-16, 3 two-pass radix-2
+  uint32_t log2_rows = 0;  // two-pass: log2 n2 (column length)
+  uint32_t tile = 0;       // two-pass: words per carry run (4 or 8)
+};
+
+// The plan for an n-word residue of exponent q.  With opt == nullptr (or all
+// zero) the policy chooses; otherwise every non-zero field is honoured or the
+// call fails with the reason in *why.
+bool make_plan(uint32_t n, uint32_t exponent, const PlanOptions* opt, Plan& plan,
+               std::string* why = nullptr);
+// Every valid explicit plan for (n, q): the autotuner's candidates.
+std::vector<PlanOptions> plan_candidates(uint32_t n, uint32_t exponent);
 
 // ------------------------------------------------------ resident kernel ----
 // One residue per CTA, state kept in shared memory for all iterations.

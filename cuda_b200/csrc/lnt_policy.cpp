@@ -80,37 +80,130 @@ static bool parse_description(const char* s, std::vector<Factor>& out) {
   return !out.empty();
 }
 
-bool make_plan(uint32_t n, Plan& plan) {
-  if (n < 2 || (n & (n - 1)) || n > (1u << kMaxLog2)) return false;
+static void name_plan(Plan& plan) {
+  if (plan.kind == PlanKind::Resident) {
+    plan.name = "RESIDENT_" + std::to_string(plan.n);
+    return;
+  }
+  plan.name = "TWOPASS_" + std::to_string(plan.n2) + "x" + std::to_string(plan.n1) +
+              (plan.fast ? "_R16" : "_R2") + "_T" + std::to_string(plan.tile);
+}
+
+// Column tiles the kernels can stage: radix-16 columns of 4096 words only fit
+// shared memory four columns wide; radix-2 columns longer than 2048 likewise.
+static bool tile_fits(bool fast, uint32_t log2n2, uint32_t tile) {
+  if (tile != 4 && tile != 8) return false;
+  if (fast) return tile == 4 || log2n2 < 12;
+  return tile == 4 || log2n2 <= 11;
+}
+
+bool make_plan(uint32_t n, uint32_t exponent, const PlanOptions* opt, Plan& plan,
+               std::string* why) {
+  auto reject = [&](const char* msg) {
+    if (why) *why = msg;
+    return false;
+  };
+  PlanOptions o = opt ? *opt : PlanOptions();
+  if (n < 2 || (n & (n - 1)) || n > (1u << kMaxLog2)) return reject("length must be 2^k, 1 <= k <= 26");
+  if (o.kind > 3) return reject("unknown plan kind");
   plan = Plan();
   plan.n = n;
   while ((1u << plan.log2n) < n) plan.log2n++;
-  if (plan.log2n <= kResidentMaxLog2) {
+  if (o.kind == 0) o.kind = plan.log2n <= kResidentMaxLog2 ? 1 : 0;
+  if (o.kind == 1) {
+    if (plan.log2n > kResidentMaxLog2) return reject("resident plan needs n <= 4096");
+    if (o.log2_rows || o.tile) return reject("resident plan takes no split or tile");
     plan.kind = PlanKind::Resident;
-    plan.name = "RESIDENT_" + std::to_string(n);
+    name_plan(plan);
     return true;
   }
+  if (plan.log2n <= kResidentMaxLog2) return reject("two-pass plans need n >= 8192");
   plan.kind = PlanKind::TwoPass;
-  uint32_t l2 = plan.log2n / 2;
-  uint32_t l1 = plan.log2n - l2;
-  if (r16_supported(l1, l2)) {
-    // radix-16 pass kernels
-    plan.fast = true;
-    plan.tile = r16_tile(l2);
-  } else {
-    if (l2 > 11) l2 = 11;
-    l1 = plan.log2n - l2;
-    if (l1 > 14) { l1 = 14; l2 = plan.log2n - 14; }
-    plan.tile = l2 <= 11 ? 8 : 4;
+  const uint32_t run_words = exponent ? r16_run_words_needed(exponent, plan.log2n) : 8;
+  uint32_t l2 = o.log2_rows, l1;
+  if (o.kind == 0) {
+    // policy: radix-16 with the most square split the kernels take
+    uint32_t p2 = plan.log2n / 2;
+    if (l2 == 0 ? r16_supported(plan.log2n - p2, p2) : r16_supported(plan.log2n - l2, l2))
+      o.kind = 2;
+    else
+      o.kind = 3;
   }
+  plan.fast = o.kind == 2;
+  if (plan.fast) {
+    if (l2 == 0) l2 = plan.log2n / 2;
+    l1 = plan.log2n - l2;
+    if (!r16_supported(l1, l2)) return reject("radix-16 plan needs 2^6 <= n2 <= n1 <= 2^12, n1 >= 2^7");
+  } else {
+    if (l2 == 0) {
+      l2 = plan.log2n / 2;
+      if (l2 > 11) l2 = 11;
+      l1 = plan.log2n - l2;
+      if (l1 > 14) { l1 = 14; l2 = plan.log2n - 14; }
+    } else {
+      l1 = plan.log2n - l2;
+    }
+    if (l2 < 1 || l1 < 1 || l1 > 14 || l2 > 12) return reject("radix-2 plan needs n1 <= 2^14, n2 <= 2^12");
+  }
+  uint32_t tile = o.tile;
+  if (tile == 0) {
+    // narrowest tile whose runs absorb every carry (more CTAs per SM)
+    tile = (run_words <= 4 && tile_fits(plan.fast, l2, 4)) ? 4 : 8;
+    if (!tile_fits(plan.fast, l2, tile)) tile = 4;
+  } else if (!tile_fits(plan.fast, l2, tile)) {
+    return reject("column tile must be 4 or 8 and fit shared memory");
+  } else if (exponent && tile < run_words && tile < 8) {
+    return reject("carry runs of this tile are too short for the exponent");
+  }
+  if ((1u << l1) < tile) return reject("rows shorter than the tile");
   plan.log2n1 = l1;
   plan.log2n2 = l2;
   plan.n1 = 1u << l1;
   plan.n2 = 1u << l2;
+  plan.tile = tile;
   plan.ntiles = plan.n1 / plan.tile;
-  plan.name = "TWOPASS_" + std::to_string(plan.n2) + "x" + std::to_string(plan.n1) +
-              (plan.fast ? "_R16" : "_R2");
+  name_plan(plan);
   return true;
+}
+
+static PlanOptions options_of(const Plan& p) {
+  PlanOptions o;
+  if (p.kind == PlanKind::Resident) {
+    o.kind = 1;
+    return o;
+  }
+  o.kind = p.fast ? 2 : 3;
+  o.log2_rows = p.log2n2;
+  o.tile = p.tile;
+  return o;
+}
+
+std::vector<PlanOptions> plan_candidates(uint32_t n, uint32_t exponent) {
+  std::vector<PlanOptions> out;
+  auto add = [&](const PlanOptions& o) {
+    for (const PlanOptions& c : out)
+      if (c.kind == o.kind && c.log2_rows == o.log2_rows && c.tile == o.tile) return;
+    out.push_back(o);
+  };
+  Plan plan;
+  if (!make_plan(n, exponent, nullptr, plan)) return out;
+  add(options_of(plan));  // the policy's plan first
+  if (plan.kind == PlanKind::Resident) return out;
+  const bool r16 = plan.fast;
+  for (uint32_t l2 = 1; l2 <= 12 && l2 < plan.log2n; ++l2)
+    for (uint32_t tile : {4u, 8u}) {
+      // radix-2 only where no radix-16 plan exists, with splits near square
+      PlanOptions o;
+      o.kind = r16 ? 2 : 3;
+      o.log2_rows = l2;
+      o.tile = tile;
+      Plan p;
+      if (!make_plan(n, exponent, &o, p)) continue;
+      const int skew = (int)p.log2n1 - (int)p.log2n2;
+      if (!r16 && (skew < 0 || skew > 3)) continue;
+      add(o);
+    }
+  return out;
 }
 
 }  // namespace lnt

@@ -20,6 +20,10 @@
 // row_square_r16: the first pass reads HBM directly (with the 4-step twiddle)
 // and the last inverse pass writes HBM directly; the last forward pass, the
 // pointwise square and the first inverse pass run in registers back to back.
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "carry.cuh"
 #include "lnt_internal.h"
 #include "ntt_core.cuh"
@@ -400,6 +404,25 @@ __global__ void __launch_bounds__(col_threads<T>(), 8 / T) col_inverse_r16(const
   tile_store(sm, ld, D.x, L, T, n1, c0);
 }
 
+// Raise a kernel's dynamic shared-memory cap once per device (the cap does not
+// change occupancy; the launch's own size does), so launches made while a
+// stream is being captured into a graph issue no attribute calls.
+template <typename K>
+cudaError_t ensure_smem(K* kernel, size_t smem) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, size_t> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(mu);
+  const auto key = std::make_pair((const void*)kernel, dev);
+  auto it = done.find(key);
+  if (it != done.end() && it->second >= smem) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) done[key] = smem;
+  return e;
+}
+
 int row_rows_per_cta(int L, int n2) {
   int rows = 4096 / L;
   if (rows < 1) rows = 1;
@@ -429,8 +452,7 @@ cudaError_t launch_row_square_r16(const TwoPassDesc& d, const TwoPassDesc* dd, u
                                   cudaStream_t s) {
   const int L = (int)d.n1, rows = row_rows_per_cta(L, (int)d.n2);
   const size_t smem = (size_t)rows * padded(L) * 8;
-  cudaError_t e = cudaFuncSetAttribute(row_square_r16, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
+  cudaError_t e = ensure_smem(row_square_r16, smem);
   if (e != cudaSuccess) return e;
   row_square_r16<<<dim3(d.n2 / rows, count), kRowThreads, smem, s>>>(dd, make_passes((int)d.log2n1),
                                                                      rows);
@@ -441,8 +463,7 @@ template <int T>
 cudaError_t col_forward_t(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count, bool apply,
                           cudaStream_t s) {
   const size_t smem = (size_t)T * col_ld((int)d.n2, T) * 8;
-  cudaError_t e = cudaFuncSetAttribute(col_forward_r16<T>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = ensure_smem(col_forward_r16<T>, smem);
   if (e != cudaSuccess) return e;
   col_forward_r16<T><<<dim3(d.ntiles, count), col_threads<T>(), smem, s>>>(
       dd, make_passes((int)d.log2n2), apply ? 1 : 0);
@@ -453,8 +474,7 @@ template <int T>
 cudaError_t col_inverse_t(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
                           bool unsigned_mode, cudaStream_t s) {
   const size_t smem = (size_t)T * col_ld((int)d.n2, T) * 8;
-  cudaError_t e = cudaFuncSetAttribute(col_inverse_r16<T>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = ensure_smem(col_inverse_r16<T>, smem);
   if (e != cudaSuccess) return e;
   col_inverse_r16<T><<<dim3(d.ntiles, count), col_threads<T>(), smem, s>>>(
       dd, make_passes((int)d.log2n2), unsigned_mode ? 1 : 0);

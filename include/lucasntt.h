@@ -73,6 +73,50 @@ int lnt_check_provided_length(uint32_t exponent, const char* description, int* d
  * and set the start value (InitializeTest, lucas_prp.cu:127-134). */
 int lnt_create(uint32_t exponent, uint32_t n, int prp, int device, lnt_test** out);
 
+/* ---- plans and autotuning ---------------------------------------------------
+ * The reference picks, per run, the fastest of its candidate lengths, pools
+ * and kernels by timing PerformanceLoops iterations of each
+ * (Process::GetBestPerformers, process.cu:45-127; KernelPool, kernel_pool.cu:17-142;
+ * LucasPRP::LucasPRP, lucas_prp.cu:36-70).  Here a plan is the kernel family,
+ * the 4-step split and the column tile of one NTT length. */
+typedef enum lnt_plan_kind {
+  LNT_PLAN_AUTO = 0,     /* the policy's choice */
+  LNT_PLAN_RESIDENT = 1, /* n <= 4096: one CTA per residue, state in shared memory (FFT_1SMEM) */
+  LNT_PLAN_RADIX16 = 2,  /* 4-step columns x rows, radix-16 register passes (FFT_2SMEM family) */
+  LNT_PLAN_RADIX2 = 3    /* 4-step columns x rows, radix-2 stages (the only one for 2^25, 2^26) */
+} lnt_plan_kind;
+
+typedef struct lnt_plan_options {
+  uint32_t kind;      /* lnt_plan_kind */
+  uint32_t log2_rows; /* two-pass: log2 of the column length n2 (n = n2 x n1); 0 = policy */
+  uint32_t tile;      /* two-pass: columns per column CTA = words per carry run, 4 or 8; 0 = policy */
+} lnt_plan_options;
+
+/* lnt_create with an explicit plan (NULL = policy): the analogue of forcing
+ * the reference's Pool / Kernels / fft options (LucasNTT.ini).  Returns
+ * LNT_ERR_UNSUPPORTED_LENGTH with the reason in lnt_last_error() for a plan the
+ * kernels cannot run, or whose carry runs are too short for the exponent. */
+int lnt_create_with_plan(uint32_t exponent, uint32_t n, int prp, int device,
+                         const lnt_plan_options* plan, lnt_test** out);
+
+/* The plan a test runs. */
+int lnt_get_plan(lnt_test* t, lnt_plan_options* out);
+
+/* KernelFactory::GetCandidates analogue (kernel_factory.cu:45-141): every valid
+ * plan for (q, n) (n = 0: policy length).  Writes min(count, cap) entries. */
+int lnt_plan_candidates(uint32_t exponent, uint32_t n, lnt_plan_options* out, int cap, int* count);
+
+/* Name of a plan ("TWOPASS_2048x4096_R16_T4"), the stats file's Pool line. */
+int lnt_plan_describe(const lnt_plan_options* plan, uint32_t exponent, uint32_t n, char* out,
+                      size_t outlen);
+
+/* Process::GetBestPerformers (process.cu:45-127): times `loops` squarings of
+ * every candidate plan (after a short warm-up) on `device`.  tried[i] / ms[i]
+ * (ms = -1: the candidate failed) for i < min(count, cap); *best indexes the
+ * fastest.  Allocates and frees one test at a time. */
+int lnt_autotune(uint32_t exponent, uint32_t n, int prp, int device, uint32_t loops,
+                 lnt_plan_options* tried, float* ms, int cap, int* count, int* best);
+
 /* LucasPRP::Finalize + ~LucasPRP (lucas_prp.cu:113-125, :74-80). NULL is ok. */
 int lnt_destroy(lnt_test* t);
 
@@ -185,6 +229,15 @@ int lnt_batch_poll(lnt_batch* b, lnt_batch_result* out, int cap, int* count);
 /* Tests in flight and device bytes they hold; tests waiting in the queue. */
 int lnt_batch_status(lnt_batch* b, uint32_t* active, uint64_t* bytes_in_use);
 int lnt_batch_pending(lnt_batch* b, uint32_t* pending);
+
+/* loops > 0: the plan of every length admitted from now on is chosen by
+ * lnt_autotune with `loops` squarings per candidate, once per length (and
+ * carry-run class) for the batch's lifetime; 0 (default): policy plans. */
+int lnt_batch_autotune(lnt_batch* b, uint32_t loops);
+
+/* enable != 0 (default): grouped squarings replay a captured CUDA graph of
+ * 8 squarings of every group; 0: plain stream launches. */
+int lnt_batch_use_graphs(lnt_batch* b, int enable);
 
 /* No counterpart in the reference.  For callers that cannot allocate device
  * memory when they need a residue in the reference's digit format (a serving

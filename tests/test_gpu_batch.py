@@ -21,9 +21,12 @@ def alone(lnt, q, n, prp, k):
         return t.res64()
 
 
-def test_batch_equals_alone(lnt):
+@pytest.mark.parametrize("graphs,tune", [(True, 0), (False, 0), (True, 20)])
+def test_batch_equals_alone(lnt, graphs, tune):
+    """Captured-graph replay, plain launches and autotuned plans all give the
+    single-test residues."""
     expected = {}
-    with lnt.Batch(device=0) as b:
+    with lnt.Batch(device=0, autotune_loops=tune, graphs=graphs) as b:
         for q, n, prp, k in MIX:
             i = b.submit(q, n, prp, k)
             expected[i] = alone(lnt, q, n, prp, k)
