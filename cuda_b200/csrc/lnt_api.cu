@@ -711,21 +711,16 @@ int lnt_plan_describe(const lnt_plan_options* o, uint32_t exponent, uint32_t n, 
 // Process::GetBestPerformers (process.cu:45-127) over this library's plans:
 // every candidate runs `loops` squarings after a short warm-up, timed with CUDA
 // events on its stream; the fastest wins.
-int lnt_autotune(uint32_t exponent, uint32_t n, int prp, int device, uint32_t loops,
-                 lnt_plan_options* tried, float* ms, int cap, int* count, int* best) {
-  if (!count || !best || (cap > 0 && (!tried || !ms))) return fail(LNT_ERR_INVALID_ARGUMENT, "null argument");
+int lnt_time_plans(uint32_t exponent, uint32_t n, int prp, int device, uint32_t loops,
+                   const lnt_plan_options* plans, int count, float* ms) {
+  if ((count > 0 && (!plans || !ms)) || count < 0) return fail(LNT_ERR_INVALID_ARGUMENT, "null argument");
   if (loops == 0) return fail(LNT_ERR_INVALID_ARGUMENT, "loops must be > 0");
   if (n == 0) n = 1u << lnt_secured_log2_length(exponent);
-  const std::vector<lnt::PlanOptions> c = lnt::plan_candidates(n, exponent);
-  *count = 0;
-  *best = -1;
-  float best_ms = 0;
-  int last_status = LNT_ERR_UNSUPPORTED_LENGTH;
-  for (size_t i = 0; i < c.size(); ++i) {
-    const lnt_plan_options o = {c[i].kind, c[i].log2_rows, c[i].tile};
+  int ok = 0, last_status = LNT_ERR_UNSUPPORTED_LENGTH;
+  for (int i = 0; i < count; ++i) {
     lnt_test* t = nullptr;
     float elapsed = -1;
-    int st = lnt_create_with_plan(exponent, n, prp, device, &o, &t);
+    int st = lnt_create_with_plan(exponent, n, prp, device, &plans[i], &t);
     if (st == LNT_OK) {
       DeviceGuard guard(t->device);
       cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -745,18 +740,80 @@ int lnt_autotune(uint32_t exponent, uint32_t n, int prp, int device, uint32_t lo
       lnt_destroy(t);
     }
     if (st == LNT_ERR_NO_DEVICE || st == LNT_ERR_CUDA) return st;
-    last_status = st;
-    if ((int)i < cap) {
-      tried[i] = o;
-      ms[i] = st == LNT_OK ? elapsed : -1.0f;
-    }
-    ++*count;
-    if (st == LNT_OK && elapsed >= 0 && (*best < 0 || elapsed < best_ms)) {
-      *best = (int)i;
-      best_ms = elapsed;
-    }
+    if (st != LNT_OK) last_status = st;
+    ms[i] = st == LNT_OK ? elapsed : -1.0f;
+    ok += st == LNT_OK;
   }
-  return *best >= 0 ? LNT_OK : last_status;
+  return ok ? LNT_OK : last_status;
+}
+
+int lnt_autotune(uint32_t exponent, uint32_t n, int prp, int device, uint32_t loops,
+                 lnt_plan_options* tried, float* ms, int cap, int* count, int* best) {
+  if (!count || !best || (cap > 0 && (!tried || !ms))) return fail(LNT_ERR_INVALID_ARGUMENT, "null argument");
+  if (n == 0) n = 1u << lnt_secured_log2_length(exponent);
+  const std::vector<lnt::PlanOptions> c = lnt::plan_candidates(n, exponent);
+  std::vector<lnt_plan_options> plans;
+  for (const auto& o : c) plans.push_back({o.kind, o.log2_rows, o.tile});
+  std::vector<float> t(plans.size(), -1.0f);
+  *count = (int)plans.size();
+  *best = -1;
+  const int st = lnt_time_plans(exponent, n, prp, device, loops, plans.data(), (int)plans.size(), t.data());
+  for (size_t i = 0; i < plans.size(); ++i) {
+    if ((int)i < cap) {
+      tried[i] = plans[i];
+      ms[i] = t[i];
+    }
+    if (t[i] >= 0 && (*best < 0 || t[i] < t[(size_t)*best])) *best = (int)i;
+  }
+  if (plans.empty()) return fail(LNT_ERR_UNSUPPORTED_LENGTH, "no plan for this length");
+  return st;
+}
+
+// LucasPRP::DumpEnvironment (lucas_prp.cu:265-291): the same lines, for the
+// host program, which has no CUDA headers of its own.
+int lnt_environment(char* out, size_t outlen) {
+  if (!out || outlen == 0) return fail(LNT_ERR_INVALID_ARGUMENT, "null argument");
+  std::string s;
+  char line[512];
+  int rt = 0;
+  cudaRuntimeGetVersion(&rt);
+  std::snprintf(line, sizeof line, "CUDA Version = %d\n", rt);
+  s += line;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess) count = 0;
+  std::snprintf(line, sizeof line, "CUDA devices = %d\n", count);
+  s += line;
+  const int kb = 1024, mb = kb * kb;
+  for (int i = 0; i < count; ++i) {
+    cudaDeviceProp p;
+    if (cudaGetDeviceProperties(&p, i) != cudaSuccess) continue;
+    std::snprintf(line, sizeof line, "Device %d = %s\n", i, p.name);
+    s += line;
+    std::snprintf(line, sizeof line, "  Revision = %d.%d\n", p.major, p.minor);
+    s += line;
+    std::snprintf(line, sizeof line, "  Multiprocessors = %d\n", p.multiProcessorCount);
+    s += line;
+    std::snprintf(line, sizeof line, "  Global memory (mb) = %d\n", (int)(p.totalGlobalMem / mb));
+    s += line;
+    std::snprintf(line, sizeof line, "  Shared memory (kb) = %d\n", (int)(p.sharedMemPerBlock / kb));
+    s += line;
+    std::snprintf(line, sizeof line, "  Constant memory (kb) = %d\n", (int)(p.totalConstMem / kb));
+    s += line;
+    std::snprintf(line, sizeof line, "  Block registers = %d\n", p.regsPerBlock);
+    s += line;
+    std::snprintf(line, sizeof line, "  Warp size = %d\n", p.warpSize);
+    s += line;
+    std::snprintf(line, sizeof line, "  Threads per block = %d\n", p.maxThreadsPerBlock);
+    s += line;
+    std::snprintf(line, sizeof line, "  Max block dimensions = [%d, %d, %d]\n", p.maxThreadsDim[0],
+                  p.maxThreadsDim[1], p.maxThreadsDim[2]);
+    s += line;
+    std::snprintf(line, sizeof line, "  Max grid dimensions = [%d, %d, %d]\n", p.maxGridSize[0],
+                  p.maxGridSize[1], p.maxGridSize[2]);
+    s += line;
+  }
+  std::snprintf(out, outlen, "%s", s.c_str());
+  return s.size() < outlen ? LNT_OK : fail(LNT_ERR_INVALID_ARGUMENT, "buffer too small");
 }
 
 int lnt_plan_name(lnt_test* t, char* out, size_t outlen) {

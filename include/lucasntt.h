@@ -117,6 +117,11 @@ int lnt_plan_describe(const lnt_plan_options* plan, uint32_t exponent, uint32_t 
 int lnt_autotune(uint32_t exponent, uint32_t n, int prp, int device, uint32_t loops,
                  lnt_plan_options* tried, float* ms, int cap, int* count, int* best);
 
+/* Process::EvaluatePerformance (process.cu:129-149) for a given list of plans:
+ * ms[i] = time of `loops` squarings with plans[i], or -1 if it failed. */
+int lnt_time_plans(uint32_t exponent, uint32_t n, int prp, int device, uint32_t loops,
+                   const lnt_plan_options* plans, int count, float* ms);
+
 /* LucasPRP::Finalize + ~LucasPRP (lucas_prp.cu:113-125, :74-80). NULL is ok. */
 int lnt_destroy(lnt_test* t);
 
@@ -148,6 +153,10 @@ int lnt_is_prime(lnt_test* t, int* is_prime);
 int lnt_get_length(lnt_test* t, uint32_t* n);
 int lnt_get_widths(lnt_test* t, uint8_t* widths, size_t n);
 int lnt_plan_name(lnt_test* t, char* out, size_t outlen);
+
+/* LucasPRP::DumpEnvironment (lucas_prp.cu:265-291): the text of the
+ * reference's .env file (CUDA version, devices and their properties). */
+int lnt_environment(char* out, size_t outlen);
 
 /* Run the test's work on a caller-owned cudaStream_t (NULL = the test's own
  * stream), the analogue of common::stream (common/common.cu:118). */

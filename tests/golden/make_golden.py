@@ -112,10 +112,12 @@ def make_ref() -> None:
             continue
         cases.append({"q": r["exponent"], "n": r["n"], "prp": r["prp"], "iterations": r["iterations"],
                       "res64": r["res64"], "fft": r["fft_used"], "pool": r["pool"],
-                      "per_iteration_ms": r["per_iteration_ms"], "conclusion": r["conclusion"]})
+                      "per_iteration_ms": r["per_iteration_ms"], "conclusion": r["conclusion"],
+                      "dump_sha256": r.get("sha256_of_dump")})
     write("ref_residues.json", {
         "source": "reference LucasNTT build (oracle/build_ref.sh) run on a B200 by oracle/run_ref.py; "
-                  "Res64 derived from its residue dump",
+                  "Res64 derived from its residue dump; dump_sha256 = SHA-256 of that dump file "
+                  "(LucasNTT_results.dat, 19-byte records)",
         "cases": cases})
 
 
