@@ -8,12 +8,14 @@ fallback: if the shared library is missing the import fails loudly.
 from __future__ import annotations
 
 import ctypes
+import os
 from pathlib import Path
 
 import numpy as np
 
 _HERE = Path(__file__).resolve().parent
-LIB_PATH = _HERE / "liblucasntt.so"
+# LUCASNTT_LIBRARY selects another build of the library (a tuned variant)
+LIB_PATH = Path(os.environ["LUCASNTT_LIBRARY"]) if os.environ.get("LUCASNTT_LIBRARY") else _HERE / "liblucasntt.so"
 HEADER = _HERE.parent / "include" / "lucasntt.h"
 
 LNT_OK = 0

@@ -26,6 +26,7 @@ constexpr int64_t kAbsorbLimit = 2;
 // for the first squaring of non-negative digits, where the reference's length
 // bound 2 n m^2 < p allows outputs above p/2.  Otherwise c is read as signed.
 GL_HD void split_output(uint64_t c, bool unsigned_mode, unsigned w, int64_t& hi, int64_t& lo) {
+  w &= 31u;  // widths are at most 30 bits (lnt_create): shifts by less than 32 are cheaper
   const uint64_t mask = (1ull << w) - 1;
   if (unsigned_mode) {
     hi = (int64_t)(c >> w);
@@ -40,6 +41,7 @@ GL_HD void split_output(uint64_t c, bool unsigned_mode, unsigned w, int64_t& hi,
 // Balanced split of t: returns the digit in [-2^(w-1), 2^(w-1)) and sets k so
 // that t = k 2^w + digit.
 GL_HD int64_t balance(int64_t t, unsigned w, int64_t& k) {
+  w &= 31u;  // as in split_output
   k = (t + (int64_t(1) << (w - 1))) >> w;
   return t - (k << w);
 }

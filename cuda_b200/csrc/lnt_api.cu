@@ -126,12 +126,38 @@ void power_table(uint32_t n, bool inverse, std::vector<uint64_t>& out) {
   for (size_t k = 1; k < n; ++k) out[k] = gl::mul(out[k - 1], r);
 }
 
-// full = false: root_table (n/2 entries); full = true: power_table (n entries)
+// Inter-pass twiddles of a length-n radix-16 transform in pass order: pass j
+// (span s, radix R, q = s / R) holds, for each task t < q, the run
+// omega_n^(t brev_R(r) n / s), r < R.  The last pass (q = 1) has none.
+void pass_table(uint32_t n, bool inverse, std::vector<uint64_t>& out) {
+  uint32_t log2n = 0;
+  while ((1u << log2n) < n) ++log2n;
+  std::vector<uint64_t> pw;
+  power_table(n, inverse, pw);
+  const std::vector<uint32_t> radix = lnt::r16_pass_radices(log2n);
+  out.clear();
+  uint32_t span = n;
+  for (size_t j = 0; j + 1 < radix.size(); ++j) {
+    const uint32_t R = radix[j], q = span / R, scale = n / span;
+    uint32_t bits = 0;
+    while ((1u << bits) < R) ++bits;
+    for (uint32_t t = 0; t < q; ++t)
+      for (uint32_t r = 0; r < R; ++r) {
+        uint32_t b = 0;
+        for (uint32_t i = 0; i < bits; ++i) b |= ((r >> i) & 1u) << (bits - 1 - i);
+        out.push_back(pw[(size_t)t * b * scale]);
+      }
+    span /= R;
+  }
+  if (out.empty()) out.push_back(1);  // keep the pointer valid
+}
+
+// full = false: root_table (n/2 entries); full = true: pass_table
 int upload_roots(lnt_test* t, uint32_t n, uint64_t** rt, uint64_t** irt, bool full = false) {
   std::vector<uint64_t> a, b;
   if (full) {
-    power_table(n, false, a);
-    power_table(n, true, b);
+    pass_table(n, false, a);
+    pass_table(n, true, b);
   } else {
     root_table(n, false, a);
     root_table(n, true, b);

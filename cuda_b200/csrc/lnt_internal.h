@@ -85,9 +85,13 @@ struct TwoPassDesc {
   const uint64_t* irt1;
   const uint64_t* rt2;    // column roots omega_n2^k, k < n2/2
   const uint64_t* irt2;
-  const uint64_t* itw1;   // radix-16 kernels: omega_n1^e, e < n1 (and inverses)
+  // radix-16 kernels: inter-pass twiddles of the row (1) and column (2)
+  // transforms, and their inverses.  Pass j of a length-L transform (span s_j,
+  // radix R_j, q_j = s_j / R_j) owns s_j words at offset s_0 + ... + s_{j-1};
+  // task t reads its R_j twiddles omega_L^(t brev(r) L / s_j) as one run.
+  const uint64_t* itw1;
   const uint64_t* iitw1;
-  const uint64_t* itw2;   // radix-16 kernels: omega_n2^e, e < n2 (and inverses)
+  const uint64_t* itw2;
   const uint64_t* iitw2;
   // radix-16 column kernels: w, uw, widths in tile-major order, index
   // (tile * n2 + row) * tile_width + column-in-tile, so a row's run is contiguous
@@ -105,6 +109,8 @@ cudaError_t launch_col_inverse(const TwoPassDesc& d, bool unsigned_mode, cudaStr
 
 // radix-16 pass variants (lnt_radix16.cu): n2 in [2^6, 2^12], n1 in [2^7, 2^12], n1 >= n2
 bool r16_supported(uint32_t log2n1, uint32_t log2n2);
+// radices of the passes of a length-2^log2L radix-16 transform, first (largest span) first
+std::vector<uint32_t> r16_pass_radices(uint32_t log2L);
 uint32_t r16_tile(uint32_t log2n2);
 uint32_t r16_run_words_needed(uint32_t exponent, uint32_t log2n);
 // `d` gives the geometry (shared by every test of the launch); `dd` is a device

@@ -55,36 +55,55 @@ Passes make_passes(int log2L) {
 
 // ---- one task: R elements of one block, forward or inverse ----------------
 
-// forward: DIF, then omega_span^(t k) (table of omega_L, scaled by L / span)
+// The R twiddles of one task, a 16-byte aligned run of the pass table: read as
+// R/2 vector loads from one base address.
+#ifndef LNT_TW_UNROLL
+#define LNT_TW_UNROLL 8  // twiddle vectors loaded per unrolled step (register pressure)
+#endif
+constexpr int kTwUnroll = LNT_TW_UNROLL;
 template <int R>
-__device__ __forceinline__ void task_dif(uint64_t* base, int off, int q, int t, const uint64_t* twL,
-                                         int tws) {
+__device__ __forceinline__ void mul_task_twiddles(uint64_t (&v)[R], const uint64_t* tw) {
+  const ulonglong2* w2 = reinterpret_cast<const ulonglong2*>(tw);
+#pragma unroll kTwUnroll
+  for (int k = 0; k < R / 2; ++k) {
+    const ulonglong2 u = __ldg(w2 + k);
+    v[2 * k] = gl::mul(v[2 * k], u.x);
+    v[2 * k + 1] = gl::mul(v[2 * k + 1], u.y);
+  }
+}
+
+// forward: DIF, then omega_span^(t k) (tw: this task's twiddles; unused when q == 1)
+template <int R>
+__device__ __forceinline__ void task_dif(uint64_t* base, int off, int q, const uint64_t* tw) {
   uint64_t v[R];
 #pragma unroll
   for (int d = 0; d < R; ++d) v[d] = base[sw(off + q * d)];
   dif<R>(v);
+  if (q > 1) mul_task_twiddles<R>(v, tw);
 #pragma unroll
-  for (int r = 0; r < R; ++r) {
-    uint64_t x = v[r];
-    if (q > 1) x = gl::mul(x, twL[t * brev_c<R>(r) * tws]);
-    base[sw(off + q * r)] = x;
-  }
+  for (int r = 0; r < R; ++r) base[sw(off + q * r)] = v[r];
 }
 
 // inverse: omega_span^-(t k), then DIT
 template <int R>
-__device__ __forceinline__ void task_dit(uint64_t* base, int off, int q, int t, const uint64_t* itwL,
-                                         int tws) {
+__device__ __forceinline__ void task_dit(uint64_t* base, int off, int q, const uint64_t* itw) {
   uint64_t v[R];
 #pragma unroll
-  for (int r = 0; r < R; ++r) {
-    uint64_t x = base[sw(off + q * r)];
-    if (q > 1) x = gl::mul(x, itwL[t * brev_c<R>(r) * tws]);
-    v[r] = x;
-  }
+  for (int r = 0; r < R; ++r) v[r] = base[sw(off + q * r)];
+  if (q > 1) mul_task_twiddles<R>(v, itw);
   dit_inv<R>(v);
 #pragma unroll
   for (int d = 0; d < R; ++d) base[sw(off + q * d)] = v[d];
+}
+
+// Offset of pass j's twiddles in a pass table (the spans of the passes before it).
+__device__ __forceinline__ int pass_table_offset(const Passes& P, int L, int j) {
+  int off = 0, span = L;
+  for (int i = 0; i < j; ++i) {
+    off += span;
+    span /= P.radix[i];
+  }
+  return off;
 }
 
 // last forward pass, pointwise square and first inverse pass (contiguous blocks)
@@ -102,10 +121,11 @@ __device__ __forceinline__ void task_square(uint64_t* base, int off) {
 }
 
 // A pass over `ntrans` transforms of length L; transform g lives at sm + g * ld.
+// tw: this pass's part of the pass table.
 template <int R, int Mode>  // Mode 0: DIF, 1: DIT, 2: square
 __device__ void pass(uint64_t* sm, int ld, int ntrans, int L, int span, const uint64_t* tw) {
   // all sizes are powers of two: index arithmetic by shifts and masks
-  const int q = span / R, per = L / R, tws = L / span;
+  const int q = span / R, per = L / R;
   const int lq = __ffs(q) - 1, lper = __ffs(per) - 1;
   const int total = ntrans * per;
   for (int task = threadIdx.x; task < total; task += blockDim.x) {
@@ -113,9 +133,9 @@ __device__ void pass(uint64_t* sm, int ld, int ntrans, int L, int span, const ui
     const int b = k >> lq, t = k & (q - 1);
     uint64_t* base = sm + g * ld;
     if constexpr (Mode == 0)
-      task_dif<R>(base, b * span + t, q, t, tw, tws);
+      task_dif<R>(base, b * span + t, q, tw + t * R);
     else if constexpr (Mode == 1)
-      task_dit<R>(base, b * span + t, q, t, tw, tws);
+      task_dit<R>(base, b * span + t, q, tw + t * R);
     else
       task_square<R>(base, b * span);
   }
@@ -135,6 +155,9 @@ __device__ __forceinline__ void pass_r(int R, uint64_t* sm, int ld, int ntrans, 
 // ------------------------------------------------------------------ rows ----
 
 constexpr int kRowThreads = 256;
+#ifndef LNT_ROW_MIN_BLOCKS
+#define LNT_ROW_MIN_BLOCKS 4  // CTAs per SM the row kernel is compiled for (registers)
+#endif
 
 // Forward pass of `rows` row transforms.  The first pass (span = L) reads HBM
 // and applies the 4-step twiddle; later passes read shared memory.  One code
@@ -143,7 +166,7 @@ template <int R>
 __device__ void row_dif_pass(uint64_t* sm, int ld, int rows, int L, int span, const uint64_t* x,
                              const uint64_t* twf, const uint64_t* twL) {
   const bool first = span == L;
-  const int q = span / R, per = L / R, tws = L / span;
+  const int q = span / R, per = L / R;
   const int lq = __ffs(q) - 1, lper = __ffs(per) - 1;
   for (int task = threadIdx.x; task < rows * per; task += blockDim.x) {
     const int g = task >> lper, k = task & (per - 1), b = k >> lq, t = k & (q - 1);
@@ -159,12 +182,9 @@ __device__ void row_dif_pass(uint64_t* sm, int ld, int rows, int L, int span, co
       for (int d = 0; d < R; ++d) v[d] = base[sw(off + q * d)];
     }
     dif<R>(v);
+    if (q > 1) mul_task_twiddles<R>(v, twL + t * R);
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      uint64_t y = v[r];
-      if (q > 1) y = gl::mul(y, twL[t * brev_c<R>(r) * tws]);
-      base[sw(off + q * r)] = y;
-    }
+    for (int r = 0; r < R; ++r) base[sw(off + q * r)] = v[r];
   }
 }
 
@@ -174,7 +194,7 @@ template <int R>
 __device__ void row_dit_pass(uint64_t* sm, int ld, int rows, int L, int span, uint64_t* x,
                              const uint64_t* twi, const uint64_t* itwL) {
   const bool last = span == L;
-  const int q = span / R, per = L / R, tws = L / span;
+  const int q = span / R, per = L / R;
   const int lq = __ffs(q) - 1, lper = __ffs(per) - 1;
   for (int task = threadIdx.x; task < rows * per; task += blockDim.x) {
     const int g = task >> lper, k = task & (per - 1), b = k >> lq, t = k & (q - 1);
@@ -182,11 +202,8 @@ __device__ void row_dit_pass(uint64_t* sm, int ld, int rows, int L, int span, ui
     uint64_t* base = sm + g * ld;
     uint64_t v[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      uint64_t y = base[sw(off + q * r)];
-      if (q > 1) y = gl::mul(y, itwL[t * brev_c<R>(r) * tws]);
-      v[r] = y;
-    }
+    for (int r = 0; r < R; ++r) v[r] = base[sw(off + q * r)];
+    if (q > 1) mul_task_twiddles<R>(v, itwL + t * R);
     dit_inv<R>(v);
     if (last) {
       const size_t rb = (size_t)g * L + off;
@@ -222,15 +239,16 @@ __device__ __forceinline__ void row_pass_r(int R, uint64_t* sm, int ld, int rows
   }
 }
 
-__global__ void __launch_bounds__(kRowThreads, 4) row_square_r16(const TwoPassDesc* __restrict__ Ds, Passes P, int rows) {
+__global__ void __launch_bounds__(kRowThreads, LNT_ROW_MIN_BLOCKS) row_square_r16(const TwoPassDesc* __restrict__ Ds, Passes P, int rows) {
   extern __shared__ __align__(16) uint64_t sm[];
   const TwoPassDesc& D = Ds[blockIdx.y];
   const int L = (int)D.n1, ld = padded(L);
   const size_t off = (size_t)blockIdx.x * rows * L;
   uint64_t* x = reinterpret_cast<uint64_t*>(D.x) + off;
   int span = L;
-  for (int j = 0; j + 1 < P.m; ++j) {
-    row_pass_r<true>(P.radix[j], sm, ld, rows, L, span, x, D.twf + off, D.itw1);
+  for (int j = 0, seg = 0; j + 1 < P.m; ++j) {
+    row_pass_r<true>(P.radix[j], sm, ld, rows, L, span, x, D.twf + off, D.itw1 + seg);
+    seg += span;
     span /= P.radix[j];
     __syncthreads();
   }
@@ -238,7 +256,8 @@ __global__ void __launch_bounds__(kRowThreads, 4) row_square_r16(const TwoPassDe
   __syncthreads();
   for (int j = P.m - 2; j >= 0; --j) {
     span *= P.radix[j];
-    row_pass_r<false>(P.radix[j], sm, ld, rows, L, span, x, D.twi + off, D.iitw1);
+    row_pass_r<false>(P.radix[j], sm, ld, rows, L, span, x, D.twi + off,
+                      D.iitw1 + pass_table_offset(P, L, j));
     if (j) __syncthreads();
   }
 }
@@ -248,6 +267,11 @@ __global__ void __launch_bounds__(kRowThreads, 4) row_square_r16(const TwoPassDe
 // column CTAs: 128 threads per tile column (T = 8: 1024 threads, T = 4: 512)
 template <int T>
 constexpr int col_threads() { return 128 * T; }
+#ifndef LNT_COL_MIN_BLOCKS
+#define LNT_COL_MIN_BLOCKS 2  // CTAs per SM the 4-column kernels are compiled for (registers)
+#endif
+template <int T>
+constexpr int col_min_blocks() { return T == 4 ? LNT_COL_MIN_BLOCKS : 1; }
 
 // column stride in words: the coalesced staging (lanes = T columns x 32/T
 // rows) then hits distinct banks
@@ -318,7 +342,7 @@ __device__ __forceinline__ void load_widths(const uint8_t* src, unsigned (&out)[
 }
 
 template <int T>
-__global__ void __launch_bounds__(col_threads<T>(), 8 / T) col_forward_r16(const TwoPassDesc* __restrict__ Ds,
+__global__ void __launch_bounds__(col_threads<T>(), col_min_blocks<T>()) col_forward_r16(const TwoPassDesc* __restrict__ Ds,
                                                                       Passes P, int apply_carries) {
   extern __shared__ __align__(16) uint64_t sm[];
   const TwoPassDesc& D = Ds[blockIdx.y];
@@ -357,8 +381,9 @@ __global__ void __launch_bounds__(col_threads<T>(), 8 / T) col_forward_r16(const
   }
   __syncthreads();
   int span = L;
-  for (int j = 0; j < P.m; ++j) {
-    pass_r<0>(P.radix[j], sm, ld, T, L, span, D.itw2);
+  for (int j = 0, seg = 0; j < P.m; ++j) {
+    pass_r<0>(P.radix[j], sm, ld, T, L, span, D.itw2 + seg);
+    seg += span;
     span /= P.radix[j];
     __syncthreads();
   }
@@ -367,7 +392,7 @@ __global__ void __launch_bounds__(col_threads<T>(), 8 / T) col_forward_r16(const
 }
 
 template <int T>
-__global__ void __launch_bounds__(col_threads<T>(), 8 / T) col_inverse_r16(const TwoPassDesc* __restrict__ Ds,
+__global__ void __launch_bounds__(col_threads<T>(), col_min_blocks<T>()) col_inverse_r16(const TwoPassDesc* __restrict__ Ds,
                                                                       Passes P, int unsigned_mode) {
   extern __shared__ __align__(16) uint64_t sm[];
   const TwoPassDesc& D = Ds[blockIdx.y];
@@ -379,7 +404,7 @@ __global__ void __launch_bounds__(col_threads<T>(), 8 / T) col_inverse_r16(const
   int span = 1;
   for (int j = P.m - 1; j >= 0; --j) {
     span *= P.radix[j];
-    pass_r<1>(P.radix[j], sm, ld, T, L, span, D.iitw2);
+    pass_r<1>(P.radix[j], sm, ld, T, L, span, D.iitw2 + pass_table_offset(P, L, j));
     __syncthreads();
   }
   // per row: unweight, carry the run of T words to balanced digits, minus two
@@ -431,6 +456,13 @@ int row_rows_per_cta(int L, int n2) {
 }
 
 }  // namespace
+
+std::vector<uint32_t> r16_pass_radices(uint32_t log2L) {
+  const Passes p = make_passes((int)log2L);
+  std::vector<uint32_t> r;
+  for (int j = 0; j < p.m; ++j) r.push_back((uint32_t)p.radix[j]);
+  return r;
+}
 
 bool r16_supported(uint32_t log2n1, uint32_t log2n2) {
   return log2n2 >= 6 && log2n2 <= 12 && log2n1 >= 7 && log2n1 <= 12 && log2n1 >= log2n2;
