@@ -50,7 +50,7 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--iterations-per-step", type=int, default=ITERATIONS_PER_STEP)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["c2", "c3", "c4", "c5"], default="c2",
+    ap.add_argument("--workload", choices=["c1", "c2", "c3", "c4", "c5"], default="c2",
                     help="c2: one 8M-point LL test (default); c3/c4: batched tests/hour; c5: serving")
     ap.add_argument("--seconds", type=float, default=30.0, help="timed window of c3/c4/c5")
     ap.add_argument("--rates", default="0.5,1,2", help="c5: arrival rates as multiples of plain capacity")
@@ -202,6 +202,26 @@ def plain_us_per_iteration(cuda_b200, exponent: int, prp: bool, iters: int = 200
         return (time.perf_counter() - t0) * 1e6 / iters
 
 
+def reference_us_per_iteration() -> dict:
+    """The reference CUDA build's own per-iteration time at each length, measured
+    on a B200 (tests/golden/ref_timings.json); its autotune keeps the fastest
+    pool, so the best run per length is its plain path."""
+    p = ROOT / "tests" / "golden" / "ref_timings.json"
+    if not p.exists():
+        return {}
+    d = json.loads(p.read_text())["by_n"]
+    return {int(n): min(r["per_iteration_us"] for r in runs) for n, runs in d.items()}
+
+
+def reference_plain_tests_per_hour(cuda_b200, exps, target_of):
+    ref = reference_us_per_iteration()
+    try:
+        t = [target_of(q) * ref[1 << cuda_b200.secured_log2_length(q)] * 1e-6 for q in exps]
+    except KeyError:
+        return None
+    return 3600 / (sum(t) / len(t))
+
+
 def run_batch_workload(args, exps, prp, target_of, label, config):
     """tests/hour of the batch engine against one-test-at-a-time, on a bounded window."""
     import cuda_b200
@@ -226,12 +246,63 @@ def run_batch_workload(args, exps, prp, target_of, label, config):
     sample = sorted(exps)[:: max(1, len(exps) // 12)]
     times = [target_of(q) * plain_us_per_iteration(cuda_b200, q, prp) * 1e-6 for q in sample]
     plain_tests_per_hour = 3600 / (sum(times) / len(times))
+    ref_plain = reference_plain_tests_per_hour(cuda_b200, exps, target_of)
     line = {"metric": f"tests/hour, {label}", "value": tests_per_hour, "unit": "tests/hour",
             "higher_is_better": True, "n_gpus": 1, "data": "synthetic (seeded exponents)",
             "dtype": "u64", "config": config,
             "plain_tests_per_hour": plain_tests_per_hour, "speedup_vs_plain": tests_per_hour / plain_tests_per_hour,
+            "reference_plain_tests_per_hour": ref_plain,
+            "speedup_vs_reference_plain": tests_per_hour / ref_plain if ref_plain else None,
             "window_s": elapsed, "squarings_per_test_in_window": steps * step,
             "plain_sample": len(sample), "finished_in_window": len(finished)}
+    print(json.dumps(line), flush=True)
+
+
+C1_EXPONENTS = [44497, 44501, 44507, 44519, 44531, 44533, 44537, 44543, 44549]
+
+
+def run_c1(args):
+    """Full LL of M_44497 and the next 8 prime exponents at the policy length
+    (2048 words): each test alone through the single-test path, then all nine
+    in one batch (one SMEM-resident launch).  Res64 checked against the
+    committed fixture of the reference build's residues."""
+    import cuda_b200
+
+    golden = json.loads((ROOT / "tests" / "golden" / "ref_residues.json").read_text())["cases"]
+    want = {c["q"]: c["res64"] for c in golden if c["n"] == 2048}
+    per_it, ok = [], True
+    with cuda_b200.LucasTest(C1_EXPONENTS[0]) as t:  # warm-up: module load, first launch
+        t.iterate(100)
+        t.synchronize()
+    t_alone = 0.0
+    for q in C1_EXPONENTS:
+        with cuda_b200.LucasTest(q) as t:
+            t0 = time.perf_counter()
+            t.iterate(q - 2)
+            r = t.res64()
+            dt = time.perf_counter() - t0
+        t_alone += dt
+        per_it.append(dt * 1e6 / (q - 2))
+        ok &= f"{r:016x}" == want.get(q, f"{r:016x}")
+    t0 = time.perf_counter()
+    with cuda_b200.Batch(device=0) as b:
+        for q in C1_EXPONENTS:
+            b.submit(q, 0, False)
+        done = []
+        while len(done) < len(C1_EXPONENTS):
+            b.run(100000)
+            done += b.poll()
+    t_batch = time.perf_counter() - t0
+    ok &= all(f"{r['res64']:016x}" == want.get(r["exponent"], f"{r['res64']:016x}") for r in done)
+    line = {"metric": "us/iteration, full LL at n=2048 (M_44497 and the next 8 primes)",
+            "value": sum(per_it) / len(per_it), "unit": "us/iteration", "higher_is_better": False,
+            "n_gpus": 1, "dtype": "u64", "data": "LL from s0 = 4 (no synthetic inputs)",
+            "config": {"workload": "C1: q = " + ",".join(map(str, C1_EXPONENTS)), "n": 2048,
+                       "plan": "RESIDENT_2048"},
+            "tests_per_hour_alone": len(C1_EXPONENTS) / t_alone * 3600,
+            "tests_per_hour_batch": len(C1_EXPONENTS) / t_batch * 3600,
+            "res64_equal_reference_build": bool(ok),
+            "reference_build_us_per_iteration": reference_us_per_iteration().get(2048)}
     print(json.dumps(line), flush=True)
 
 
@@ -311,6 +382,10 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
+    if args.workload == "c1":
+        if rank == 0:
+            run_c1(args)
+        return
     if args.workload in ("c3", "c4", "c5"):
         import random
 
@@ -365,15 +440,24 @@ def main():
     barrier()
     clocks = ClockSampler(local_rank)
     clocks.start()
+    # headline: the production path (lnt_iterate, captured-graph replay), CUDA
+    # events on the test's stream around each step
     step_ms, kernels = [], {}
-    for _ in range(args.steps):
+    ev_a = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev_b = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    for k in range(args.steps):
         flush_l2()
-        prof = test.profile_iterations(ips)  # CUDA events between the launches
-        step_ms.append(sum(ms for _, ms in prof.values()))
-        for name, (launches, ms) in prof.items():
-            a = kernels.setdefault(name, [0, 0.0])
-            a[0] += launches
-            a[1] += ms
+        ev_a[k].record(stream)
+        test.iterate(ips)
+        ev_b[k].record(stream)
+    stream.synchronize()
+    step_ms = [a.elapsed_time(b) for a, b in zip(ev_a, ev_b)]
+    # per-kernel breakdown (roofline): one more step of the same work with CUDA
+    # events between the launches, inside the same sampled region
+    flush_l2()
+    prof = test.profile_iterations(ips)
+    for name, (launches, ms) in prof.items():
+        kernels[name] = [launches, ms]
     torch.cuda.synchronize(dev)
     clk = clocks.stop()
     barrier()
@@ -420,7 +504,8 @@ def main():
     achieved = algo_bytes / avg_s / 1e9
     peak, peak_kind = measured_peak_hbm()
     traffic = ncu_traffic(dom_name)
-    launches_in_timed = sum(a[0] for a in kernels.values())
+    # every timed step launches the same kernels as the profiled one
+    launches_in_timed = sum(a[0] for a in kernels.values()) * (args.steps + 1)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -438,7 +523,10 @@ def main():
             "config": {"workload": f"LL q={EXPONENT} n=2^{LOG2N} (8M-pt NTT), {ips} squarings per step",
                        "exponent": EXPONENT, "n": N, "iterations_per_step": ips, "plan": test.plan,
                        "parallelism": "replicas" if world > 1 else "single",
-                       "l2": "flushed between steps (256 MiB write)", "res64_after_run": f"{res64:016x}"},
+                       "l2": "flushed between steps (256 MiB write)", "res64_after_run": f"{res64:016x}",
+                       "timing": "value: CUDA events around lnt_iterate per step (graph replay); kernels: "
+                                 "one more step with events between launches",
+                       "reference_build_us_per_iteration": reference_us_per_iteration().get(N)},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": N * 8, "d2h_bytes_per_step": N * 8,
                     "wall_s": wall},
             "gpu_launches": launches_in_timed,

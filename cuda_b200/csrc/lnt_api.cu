@@ -57,6 +57,9 @@ struct lnt_test {
   bool pristine = true;         // no squaring since the digits were set
   bool zero_start = false;      // digits were set to all zero
   bool canon_valid = false;     // `canon` holds the canonical digits of the current state
+  // steady-state squarings of the pass-kernel plan, captured once and replayed
+  cudaGraphExec_t graph = nullptr;
+  bool graph_failed = false;    // capture unavailable on this stream: plain launches
 };
 
 namespace {
@@ -104,6 +107,7 @@ void free_all(lnt_test* t) {
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (t->h_pinned) cudaFreeHost(t->h_pinned);
+  if (t->graph) cudaGraphExecDestroy(t->graph);
   if (t->own_stream && t->stream) cudaStreamDestroy(t->stream);
 }
 
@@ -359,6 +363,30 @@ struct LaunchTimer {
   } while (0)
 
 // Queue `iterations` squarings on the test's stream (LucasPRP::MainLoop).
+// Squarings per captured graph: launch overhead amortised over 3 x 16 kernels.
+constexpr uint64_t kGraphSquarings = 16;
+
+// Capture kGraphSquarings steady-state squarings of a pass-kernel test on its
+// stream.  On any failure the test keeps plain launches (graph_failed).
+void capture_graph(lnt_test* t, const lnt::TwoPassDesc& d) {
+  cudaGraph_t g = nullptr;
+  if (cudaStreamBeginCapture(t->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    t->graph_failed = true;
+    return;
+  }
+  bool ok = true;
+  for (uint64_t k = 0; k < kGraphSquarings && ok; ++k)
+    ok = lnt::launch_col_forward_r16(d, t->tdesc, 1, true, t->stream) == cudaSuccess &&
+         lnt::launch_row_square_r16(d, t->tdesc, 1, t->stream) == cudaSuccess &&
+         lnt::launch_col_inverse_r16(d, t->tdesc, 1, false, t->stream) == cudaSuccess;
+  const cudaError_t e = cudaStreamEndCapture(t->stream, &g);
+  if (ok && e == cudaSuccess && g && cudaGraphInstantiate(&t->graph, g, 0) != cudaSuccess) t->graph = nullptr;
+  if (g) cudaGraphDestroy(g);
+  cudaGetLastError();  // a failed capture leaves no error behind for the next launch
+  if (!t->graph) t->graph_failed = true;
+}
+
 int queue_iterations(lnt_test* t, uint64_t iterations, LaunchTimer* timer) {
   if (t->plan.kind == lnt::PlanKind::Resident) {
     lnt::ResidentDesc d{};
@@ -381,7 +409,18 @@ int queue_iterations(lnt_test* t, uint64_t iterations, LaunchTimer* timer) {
     LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
   } else {
     lnt::TwoPassDesc d = twopass_desc(t);
-    for (uint64_t i = 0; i < iterations; ++i) {
+    uint64_t i = 0;
+    // steady state (carries pending, signed outputs): whole chunks replay a graph
+    auto steady = [&]() { return t->pending_carries && !t->canonical_input; };
+    for (; i < iterations; ++i) {
+      if (t->plan.fast && !timer && steady() && iterations - i >= kGraphSquarings && !t->graph_failed) {
+        if (!t->graph) capture_graph(t, d);
+        if (t->graph) {
+          for (; iterations - i >= kGraphSquarings; i += kGraphSquarings)
+            LNT_CUDA(cudaGraphLaunch(t->graph, t->stream), "graph launch");
+          if (i == iterations) break;
+        }
+      }
       if (t->plan.fast) {
         LNT_LAUNCH(lnt::launch_col_forward_r16(d, t->tdesc, 1, t->pending_carries, t->stream),
                    "col_forward");

@@ -109,8 +109,10 @@ cudaError_t launch_col_inverse(const TwoPassDesc& d, bool unsigned_mode, cudaStr
 
 // radix-16 pass variants (lnt_radix16.cu): n2 in [2^6, 2^12], n1 in [2^7, 2^12], n1 >= n2
 bool r16_supported(uint32_t log2n1, uint32_t log2n2);
-// radices of the passes of a length-2^log2L radix-16 transform, first (largest span) first
+// radices of the passes of a length-2^log2L transform, first (largest span) first,
+// and the largest radix the kernels were built with (8 or 16)
 std::vector<uint32_t> r16_pass_radices(uint32_t log2L);
+uint32_t r16_max_radix();
 uint32_t r16_tile(uint32_t log2n2);
 uint32_t r16_run_words_needed(uint32_t exponent, uint32_t log2n);
 // `d` gives the geometry (shared by every test of the launch); `dd` is a device

@@ -86,7 +86,7 @@ static void name_plan(Plan& plan) {
     return;
   }
   plan.name = "TWOPASS_" + std::to_string(plan.n2) + "x" + std::to_string(plan.n1) +
-              (plan.fast ? "_R16" : "_R2") + "_T" + std::to_string(plan.tile);
+              (plan.fast ? "_R" + std::to_string(r16_max_radix()) : std::string("_R2")) + "_T" + std::to_string(plan.tile);
 }
 
 // Column tiles the kernels can stage: radix-16 columns of 4096 words only fit
@@ -123,7 +123,7 @@ bool make_plan(uint32_t n, uint32_t exponent, const PlanOptions* opt, Plan& plan
   uint32_t l2 = o.log2_rows, l1;
   if (o.kind == 0) {
     // policy: radix-16 with the most square split the kernels take
-    uint32_t p2 = plan.log2n / 2;
+    const uint32_t p2 = plan.log2n / 2 < 12 ? plan.log2n / 2 : 12;
     if (l2 == 0 ? r16_supported(plan.log2n - p2, p2) : r16_supported(plan.log2n - l2, l2))
       o.kind = 2;
     else
@@ -131,7 +131,7 @@ bool make_plan(uint32_t n, uint32_t exponent, const PlanOptions* opt, Plan& plan
   }
   plan.fast = o.kind == 2;
   if (plan.fast) {
-    if (l2 == 0) l2 = plan.log2n / 2;
+    if (l2 == 0) l2 = plan.log2n / 2 < 12 ? plan.log2n / 2 : 12;
     l1 = plan.log2n - l2;
     if (!r16_supported(l1, l2)) return reject("radix-16 plan needs 2^6 <= n2 <= n1 <= 2^12, n1 >= 2^7");
   } else {

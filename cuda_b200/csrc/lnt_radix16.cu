@@ -1,4 +1,4 @@
-// Two-pass squaring with radix-16 register passes (n = 2^13 ... 2^24).
+// Two-pass squaring with register passes of radix up to 16 (n = 2^13 ... 2^24).
 //
 // Same layout, twiddle tables and carry scheme as lnt_twopass.cu (which
 // replaces the reference's FFT_2SMEM pool, kernel_pool.cu:39-48).  A transform
@@ -37,19 +37,29 @@ __host__ __device__ constexpr int padded(int L) { return L + L / 16; }
 
 struct Passes {
   int m;          // number of passes
-  int radix[4];   // r_0 (largest stride) ... r_{m-1} (contiguous)
+  int radix[6];   // r_0 (largest stride) ... r_{m-1} (contiguous)
 };
 
+// Largest pass radix.  8 (three radix-2 stages per pass) keeps a task's values,
+// twiddles and addresses within the 64 registers that four row CTAs (two column
+// CTAs) per SM allow; 16 needs one twiddle stage less per direction but spills
+// (measured at n = 2^23: 561 us per squaring with 8, 574 with 16).
+#ifndef LNT_MAX_RADIX_LOG2
+#define LNT_MAX_RADIX_LOG2 3
+#endif
+constexpr int kMaxRadix = 1 << LNT_MAX_RADIX_LOG2;
+
 Passes make_passes(int log2L) {
+  constexpr int b = LNT_MAX_RADIX_LOG2;
   Passes p{};
-  int first = log2L % 4;
+  int first = log2L % b;
   int rest = log2L - first;
   if (first == 0) {
-    first = 4;
-    rest -= 4;
+    first = b;
+    rest -= b;
   }
   p.radix[p.m++] = 1 << first;
-  for (int k = 0; k < rest / 4; ++k) p.radix[p.m++] = 16;
+  for (int k = 0; k < rest / b; ++k) p.radix[p.m++] = 1 << b;
   return p;
 }
 
@@ -148,7 +158,7 @@ __device__ __forceinline__ void pass_r(int R, uint64_t* sm, int ld, int ntrans, 
     case 2: pass<2, Mode>(sm, ld, ntrans, L, span, tw); break;
     case 4: pass<4, Mode>(sm, ld, ntrans, L, span, tw); break;
     case 8: pass<8, Mode>(sm, ld, ntrans, L, span, tw); break;
-    default: pass<16, Mode>(sm, ld, ntrans, L, span, tw); break;
+    default: pass<kMaxRadix, Mode>(sm, ld, ntrans, L, span, tw); break;
   }
 }
 
@@ -233,8 +243,8 @@ __device__ __forceinline__ void row_pass_r(int R, uint64_t* sm, int ld, int rows
       else row_dit_pass<8>(sm, ld, rows, L, span, x, tw4, twL);
       break;
     default:
-      if constexpr (Forward) row_dif_pass<16>(sm, ld, rows, L, span, x, tw4, twL);
-      else row_dit_pass<16>(sm, ld, rows, L, span, x, tw4, twL);
+      if constexpr (Forward) row_dif_pass<kMaxRadix>(sm, ld, rows, L, span, x, tw4, twL);
+      else row_dit_pass<kMaxRadix>(sm, ld, rows, L, span, x, tw4, twL);
       break;
   }
 }
@@ -457,6 +467,8 @@ int row_rows_per_cta(int L, int n2) {
 
 }  // namespace
 
+uint32_t r16_max_radix() { return (uint32_t)kMaxRadix; }
+
 std::vector<uint32_t> r16_pass_radices(uint32_t log2L) {
   const Passes p = make_passes((int)log2L);
   std::vector<uint32_t> r;
@@ -464,8 +476,12 @@ std::vector<uint32_t> r16_pass_radices(uint32_t log2L) {
   return r;
 }
 
+// Rows up to 2^14 words (139 KB of shared memory, one CTA per SM) and columns
+// up to 2^12 (four columns: 139 KB): with B200's 227 KB per CTA the 2^25 and
+// 2^26 lengths stay two-pass, where the reference needs 3-factor plans
+// (ntt_lengths.cu:118-127).
 bool r16_supported(uint32_t log2n1, uint32_t log2n2) {
-  return log2n2 >= 6 && log2n2 <= 12 && log2n1 >= 7 && log2n1 <= 12 && log2n1 >= log2n2;
+  return log2n2 >= 6 && log2n2 <= 12 && log2n1 >= 7 && log2n1 <= 14 && log2n1 >= log2n2;
 }
 
 uint32_t r16_tile(uint32_t log2n2) { return log2n2 >= 12 ? 4 : 8; }

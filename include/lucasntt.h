@@ -82,7 +82,7 @@ int lnt_create(uint32_t exponent, uint32_t n, int prp, int device, lnt_test** ou
 typedef enum lnt_plan_kind {
   LNT_PLAN_AUTO = 0,     /* the policy's choice */
   LNT_PLAN_RESIDENT = 1, /* n <= 4096: one CTA per residue, state in shared memory (FFT_1SMEM) */
-  LNT_PLAN_RADIX16 = 2,  /* 4-step columns x rows, radix-16 register passes (FFT_2SMEM family) */
+  LNT_PLAN_RADIX16 = 2,  /* 4-step columns x rows, register passes of radix <= 16 (FFT_2SMEM family) */
   LNT_PLAN_RADIX2 = 3    /* 4-step columns x rows, radix-2 stages (the only one for 2^25, 2^26) */
 } lnt_plan_kind;
 
@@ -106,7 +106,8 @@ int lnt_get_plan(lnt_test* t, lnt_plan_options* out);
  * plan for (q, n) (n = 0: policy length).  Writes min(count, cap) entries. */
 int lnt_plan_candidates(uint32_t exponent, uint32_t n, lnt_plan_options* out, int cap, int* count);
 
-/* Name of a plan ("TWOPASS_2048x4096_R16_T4"), the stats file's Pool line. */
+/* Name of a plan ("TWOPASS_2048x4096_R8_T4": n2 x n1, pass radix, tile), the
+ * stats file's Pool line. */
 int lnt_plan_describe(const lnt_plan_options* plan, uint32_t exponent, uint32_t n, char* out,
                       size_t outlen);
 

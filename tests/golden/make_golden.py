@@ -121,6 +121,24 @@ def make_ref() -> None:
         "cases": cases})
 
 
+def make_ref_timings() -> None:
+    """Per-iteration times of the reference build at each NTT length, from the
+    oracle/run_ref.py summaries collected on a B200 (gpurun_out/ref_*/run_*.json).
+    bench.py uses them to state the reference's plain one-at-a-time tests/hour."""
+    base = ROOT / "gpurun_out"
+    by_n = {}
+    for js in sorted(base.glob("ref_*/run_*.json")):
+        r = json.loads(js.read_text())
+        if r.get("rc") != 0 or not r.get("per_iteration_ms"):
+            continue
+        by_n.setdefault(str(r["n"]), []).append({"q": r["exponent"], "prp": r["prp"], "pool": r["pool"],
+                                                 "fft": r["fft_used"], "per_iteration_us": r["per_iteration_ms"] * 1e3})
+    write("ref_timings.json", {
+        "source": "reference LucasNTT build (oracle/build_ref.sh) run on a B200 by oracle/run_ref.py; "
+                  "its own 'Per iteration (ms)' (lucas_prp.cu:319)",
+        "by_n": by_n})
+
+
 if __name__ == "__main__":
     sets = sys.argv[1:] or ["small"]
     for s in sets:
@@ -132,3 +150,5 @@ if __name__ == "__main__":
             make_c2("--c2-long" in sets)
         elif s == "ref":
             make_ref()
+        elif s == "reftimes":
+            make_ref_timings()

@@ -184,7 +184,8 @@ def test_provided_length_prompt(tmp_path):
     assert r.returncode == 0 and stats(tmp_path / "x.txt")["n"] == "4096"
 
 
-def test_pool_preference(tmp_path):
-    r = run_cli(tmp_path, [1000003, 200, "p"], ini="PerformanceLoops = 50\nPool = TWOPASS_128x512_R16_T8\n")
+def test_pool_preference(tmp_path, lnt):
+    name = lnt.plan_describe((2, 7, 8), 1000003)  # a plan the policy would not pick
+    r = run_cli(tmp_path, [1000003, 200, "p"], ini=f"PerformanceLoops = 50\nPool = {name}\n")
     assert r.returncode == 0, r.stdout
-    assert stats(tmp_path / "p.txt")["Pool"] == "TWOPASS_128x512_R16_T8"
+    assert stats(tmp_path / "p.txt")["Pool"] == name

@@ -4,7 +4,7 @@ The reference's autotune times several pools and kernels per length and keeps
 the fastest (process.cu:45-127); any of them must produce the same residue.
 Here each candidate plan (4-step split, column tile, radix-16 or radix-2
 kernels) is run from the same random state and compared digit for digit
-with the oracle, including the radix-2 plans of 2^25 and 2^26 words.
+with the oracle, including the largest lengths, 2^25 and 2^26 words.
 """
 import numpy as np
 import pytest
@@ -52,13 +52,17 @@ def test_every_candidate_plan_matches_oracle(lnt, oracle_mod, q, n, prp):
 
 
 @pytest.mark.parametrize("q", [600000001, 1100000009])
-def test_radix2_largest_lengths(lnt, oracle_mod, q):
-    """2^25 and 2^26 words (the radix-2 plans): one squaring from a random state."""
+def test_largest_lengths(lnt, oracle_mod, q):
+    """2^25 and 2^26 words: the policy's pass-kernel plan (rows of 8K / 16K words)
+    and the radix-2 plan, one squaring from a random state, against the oracle."""
     n = 1 << lnt.secured_log2_length(q)
     start = random_digits(q, n, 11)
     want = oracle_digits(oracle_mod, q, n, False, start, 1)
     got, name = run_plan(lnt, q, n, False, (0, 0, 0), start, 1)
-    assert "R2" in name
+    assert name.startswith("TWOPASS_4096x") and "_R2" not in name
+    assert np.array_equal(got, want)
+    got, name = run_plan(lnt, q, n, False, (3, 12, 4), start, 1)
+    assert "_R2" in name
     assert np.array_equal(got, want)
 
 
