@@ -189,11 +189,9 @@ def primes_between(lo: int, hi: int) -> list[int]:
     return [int(x) for x in np.nonzero(sieve)[0] if x >= lo]
 
 
-def plain_us_per_iteration(cuda_b200, exponent: int, prp: bool, iters: int = 200) -> float:
+def plain_us_per_iteration(cuda_b200, exponent: int, prp: bool, iters: int = 200, device: int = 0) -> float:
     """One test alone through the single-test path (the reference's way)."""
-    import torch
-
-    with cuda_b200.LucasTest(exponent, 0, prp) as t:
+    with cuda_b200.LucasTest(exponent, 0, prp, device=device) as t:
         t.iterate(20)
         t.synchronize()
         t0 = time.perf_counter()
@@ -222,17 +220,32 @@ def reference_plain_tests_per_hour(cuda_b200, exps, target_of):
     return 3600 / (sum(t) / len(t))
 
 
-def run_batch_workload(args, exps, prp, target_of, label, config):
-    """tests/hour of the batch engine against one-test-at-a-time, on a bounded window."""
+def run_batch_workload(args, exps, prp, target_of, label, config, rank=0, world=1, local_rank=0):
+    """tests/hour of the batch engine against one-test-at-a-time, on a bounded
+    window.  With N ranks (one process per GPU) each rank runs its own batch over
+    a cost-balanced share of the work list (cuda_b200/shard.py) and rank 0
+    reports the whole job: the tests all ranks advanced over the slowest rank's
+    window.  No collective touches the data path."""
     import cuda_b200
+    from cuda_b200 import shard
 
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    mine = shard.partition_by_cost(exps, world, lambda q: shard.test_cost(q, target_of(q), prp))[rank]
     step = 50
-    with cuda_b200.Batch(device=0) as b:
-        ids = {}
-        for q in exps:
-            ids[b.submit(q, 0, prp, target_of(q))] = q
+    with cuda_b200.Batch(device=local_rank) as b:
+        for q in mine:
+            b.submit(q, 0, prp, target_of(q))
         for _ in range(3):
             b.run(step)
+        if dist is not None:
+            dist.barrier()
         steps = 0
         t0 = time.perf_counter()
         while time.perf_counter() - t0 < args.seconds:
@@ -240,22 +253,33 @@ def run_batch_workload(args, exps, prp, target_of, label, config):
             steps += 1
         elapsed = time.perf_counter() - t0
         finished = b.poll()
-    done_fraction = sum(min(1.0, steps * step / target_of(q)) for q in exps)
-    tests_per_hour = done_fraction / elapsed * 3600
-    # plain path: a sample spread over the exponents, each test alone
-    sample = sorted(exps)[:: max(1, len(exps) // 12)]
-    times = [target_of(q) * plain_us_per_iteration(cuda_b200, q, prp) * 1e-6 for q in sample]
-    plain_tests_per_hour = 3600 / (sum(times) / len(times))
-    ref_plain = reference_plain_tests_per_hour(cuda_b200, exps, target_of)
-    line = {"metric": f"tests/hour, {label}", "value": tests_per_hour, "unit": "tests/hour",
-            "higher_is_better": True, "n_gpus": 1, "data": "synthetic (seeded exponents)",
-            "dtype": "u64", "config": config,
-            "plain_tests_per_hour": plain_tests_per_hour, "speedup_vs_plain": tests_per_hour / plain_tests_per_hour,
-            "reference_plain_tests_per_hour": ref_plain,
-            "speedup_vs_reference_plain": tests_per_hour / ref_plain if ref_plain else None,
-            "window_s": elapsed, "squarings_per_test_in_window": steps * step,
-            "plain_sample": len(sample), "finished_in_window": len(finished)}
-    print(json.dumps(line), flush=True)
+    done_local = sum(min(1.0, steps * step / target_of(q)) for q in mine)
+    done = sum(shard.gather_results([done_local], dist))
+    elapsed = shard.max_over_ranks(elapsed, dist)
+    n_finished = sum(shard.gather_results([len(finished)], dist))
+    tests_per_hour = done / elapsed * 3600
+    plain_tests_per_hour = ref_plain = None
+    if rank == 0:
+        # plain path: a sample spread over the exponents, each test alone on one GPU
+        sample = sorted(exps)[:: max(1, len(exps) // 12)]
+        times = [target_of(q) * plain_us_per_iteration(cuda_b200, q, prp, device=local_rank) * 1e-6
+                 for q in sample]
+        plain_tests_per_hour = 3600 / (sum(times) / len(times))
+        ref_plain = reference_plain_tests_per_hour(cuda_b200, exps, target_of)
+        line = {"metric": f"tests/hour, {label}", "value": tests_per_hour, "unit": "tests/hour",
+                "higher_is_better": True, "n_gpus": world, "data": "synthetic (seeded exponents)",
+                "dtype": "u64", "config": config,
+                "scaling": "strong" if world > 1 else "weak",
+                "plain_tests_per_hour": plain_tests_per_hour,
+                "speedup_vs_plain": tests_per_hour / plain_tests_per_hour,
+                "reference_plain_tests_per_hour": ref_plain,
+                "speedup_vs_reference_plain": tests_per_hour / ref_plain if ref_plain else None,
+                "window_s": elapsed, "squarings_per_test_in_window": steps * step,
+                "plain_sample": len(sample), "finished_in_window": n_finished}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 C1_EXPONENTS = [44497, 44501, 44507, 44519, 44531, 44533, 44537, 44543, 44549]
@@ -306,15 +330,28 @@ def run_c1(args):
     print(json.dumps(line), flush=True)
 
 
-def run_serving(args):
+def run_serving(args, rank=0, world=1, local_rank=0):
     """Poisson stream of LL/PRP requests against the continuous-batching engine,
-    beside the plain sequential path (a FIFO queue over measured service times)."""
+    beside the plain sequential path (a FIFO queue over measured service times).
+    With N ranks the stream's rate is N times higher and request i goes to rank
+    i mod N (round-robin dispatch to one engine per GPU); rank 0 reports the
+    percentiles over all ranks' latencies."""
     import math
     import random
 
     import numpy as np
 
     import cuda_b200
+    from cuda_b200 import shard
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
 
     lo, hi = (int(x) for x in args.c5_range.split(","))
     primes = primes_between(lo, min(hi * 2, hi + 100000))
@@ -326,13 +363,13 @@ def run_serving(args):
         return primes[min(bisect.bisect_left(primes, int(x)), len(primes) - 1)], rng.random() < 0.5
 
     pool = [draw() for _ in range(64)]
-    service = [(q if prp else q - 2) * plain_us_per_iteration(cuda_b200, q, prp, 100) * 1e-6
+    service = [(q if prp else q - 2) * plain_us_per_iteration(cuda_b200, q, prp, 100, local_rank) * 1e-6
                for q, prp in pool[:16]]
     mean_service = sum(service) / len(service)
     plain_capacity = 1.0 / mean_service  # tests per second, one at a time
     budget = 150 << 30
     for mult in (float(r) for r in args.rates.split(",")):
-        rate = mult * plain_capacity
+        rate = mult * plain_capacity * world
         t = 0.0
         arrivals = []
         while t < args.seconds:
@@ -340,8 +377,12 @@ def run_serving(args):
             q, prp = pool[rng.randrange(len(pool))]
             arrivals.append((t, q, prp))
         arrivals = [a for a in arrivals if a[0] < args.seconds]
+        all_arrivals = arrivals
+        arrivals = arrivals[rank::world]
         lat, done = [], 0
-        with cuda_b200.Batch(device=0, hbm_budget_bytes=budget) as b:
+        if dist is not None:
+            dist.barrier()
+        with cuda_b200.Batch(device=local_rank, hbm_budget_bytes=budget) as b:
             t0 = time.perf_counter()
             k, enq = 0, {}
             while (k < len(arrivals) or done < len(arrivals)) and time.perf_counter() - t0 < 4 * args.seconds:
@@ -355,25 +396,35 @@ def run_serving(args):
                     lat.append(r["seconds"] + enq.pop(r["id"], 0.0))
                     done += 1
             wall = time.perf_counter() - t0
-        # plain sequential path: FIFO over the same arrivals, service = measured per-test time
+        lat = shard.gather_results(lat, dist)
+        done = sum(shard.gather_results([done], dist))
+        wall = shard.max_over_ranks(wall, dist)
+        if rank != 0:
+            continue
+        # plain sequential path: one GPU, FIFO over the same arrivals, service =
+        # measured per-test time
         serv = {}
         free_at, plain_lat = 0.0, []
-        for (ta, q, prp) in arrivals:
+        for (ta, q, prp) in all_arrivals:
             if (q, prp) not in serv:
-                serv[(q, prp)] = (q if prp else q - 2) * plain_us_per_iteration(cuda_b200, q, prp, 100) * 1e-6
+                serv[(q, prp)] = (q if prp else q - 2) * plain_us_per_iteration(cuda_b200, q, prp, 100, local_rank) * 1e-6
             start = max(free_at, ta)
             free_at = start + serv[(q, prp)]
             plain_lat.append(free_at - ta)
         line = {"metric": "serving p50/p99 latency and tests/hour", "rate_multiple_of_plain_capacity": mult,
-                "requests": len(arrivals), "completed": done, "wall_s": wall,
+                "requests": len(all_arrivals), "completed": done, "wall_s": wall, "n_gpus": world,
                 "p50_s": float(np.percentile(lat, 50)) if lat else None,
                 "p99_s": float(np.percentile(lat, 99)) if lat else None,
                 "tests_per_hour": done / wall * 3600,
                 "plain_p50_s": float(np.percentile(plain_lat, 50)), "plain_p99_s": float(np.percentile(plain_lat, 99)),
-                "plain_tests_per_hour": len(arrivals) / free_at * 3600 if free_at else None,
+                "plain_tests_per_hour": len(all_arrivals) / free_at * 3600 if free_at else None,
                 "config": {"exponents": f"primes log-uniform in [{lo}, {hi}], LL/PRP by a seeded coin (seed 2)",
-                           "hbm_budget_gb": 150, "arrival": "Poisson"}}
+                           "hbm_budget_gb": 150, "arrival": "Poisson",
+                           "dispatch": "round-robin over ranks" if world > 1 else "one engine"}}
         print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def main():
@@ -392,13 +443,15 @@ def main():
         if args.workload == "c3":
             exps = random.Random(0).sample(primes_between(100000, 2000000), 256)
             run_batch_workload(args, exps, False, lambda q: q - 2, "256 full LL tests, q in [1e5, 2e6] (seed 0)",
-                               {"workload": "C3 batch", "count": 256, "lengths": "4K-128K"})
+                               {"workload": "C3 batch", "count": 256, "lengths": "4K-128K"},
+                               rank, world, local_rank)
         elif args.workload == "c4":
             exps = random.Random(1).sample(primes_between(5000000, 20000000), 64)
             run_batch_workload(args, exps, True, lambda q: 20000, "64 PRP tests x 20000 squarings, q in [5e6, 2e7] (seed 1)",
-                               {"workload": "C4 batch", "count": 64, "lengths": "512K-1M"})
+                               {"workload": "C4 batch", "count": 64, "lengths": "512K-1M"},
+                               rank, world, local_rank)
         else:
-            run_serving(args)
+            run_serving(args, rank, world, local_rank)
         return
 
     import torch

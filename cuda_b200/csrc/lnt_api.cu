@@ -583,7 +583,7 @@ int lnt_create_with_plan(uint32_t exponent, uint32_t n, int prp, int device,
 
   int st;
   if (plan.kind == lnt::PlanKind::Resident) {
-    if ((st = upload_roots(t, n, &t->rt, &t->irt)) != LNT_OK) return bail(st);
+    if ((st = upload_roots(t, n, &t->rt, &t->irt, true)) != LNT_OK) return bail(st);
     if ((e = dalloc(&t->rdesc, 1))) return bail(cuda_fail(e, "allocate descriptor"));
   } else {
     if ((st = upload_roots(t, plan.n1, &t->rt1, &t->irt1)) != LNT_OK) return bail(st);

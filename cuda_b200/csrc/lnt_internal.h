@@ -58,8 +58,8 @@ struct ResidentDesc {
   const uint64_t* w;      // IBDWT weights
   const uint64_t* uw;     // unweights with 1/n folded in
   const uint8_t* widths;  // digit widths
-  const uint64_t* rt;     // omega_n^k, k < n/2
-  const uint64_t* irt;    // omega_n^-k
+  const uint64_t* rt;     // pass table of the length-n transform (smem_passes.cuh)
+  const uint64_t* irt;    // and of its inverse
   uint32_t* status;
   uint32_t n, log2n;
   uint32_t prp;
@@ -68,7 +68,7 @@ struct ResidentDesc {
 };
 
 size_t resident_smem_bytes(uint32_t n, uint32_t threads);
-uint32_t resident_threads(uint32_t n);
+uint32_t resident_threads(uint32_t n, uint32_t count);
 cudaError_t launch_resident(const ResidentDesc* d_descs, uint32_t count, uint32_t max_n,
                             cudaStream_t stream);
 

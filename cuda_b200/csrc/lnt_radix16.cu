@@ -1,21 +1,10 @@
-// Two-pass squaring with register passes of radix up to 16 (n = 2^13 ... 2^24).
+// Two-pass squaring with register passes (smem_passes.cuh) for n = 2^13 ... 2^26.
 //
 // Same layout, twiddle tables and carry scheme as lnt_twopass.cu (which
-// replaces the reference's FFT_2SMEM pool, kernel_pool.cu:39-48).  A transform
-// of length L = r0 * r1 * ... (every r <= 16, a power of two) runs as passes
-// over shared memory: pass j takes R = r_j elements at stride span_j / R from a
-// block of span_j = L / (r0 ... r_{j-1}) words into registers, does an R-point
-// DIF with power-of-two twiddles (ntt_core.cuh), multiplies by
-// omega_span^(t * k) and writes back.  The result is in fully bit-reversed order,
-// like the radix-2 kernels, so all plans share the 4-step twiddle tables.
-// Per element a pass costs log2(R) shift butterflies and one table
-// multiplication; the reference pays one general modular multiplication per
-// radix-2 butterfly (core/fft_r2.cuh:17-107).
-//
-// Small unrolled bodies (one 16-point transform) inside runtime loops keep the
-// kernels small enough for the instruction cache; fully unrolled 64-point
-// passes starved the SM of instructions.  Shared memory is padded by one word
-// in 16 (sw below), which makes every pass stride bank-conflict free.
+// replaces the reference's FFT_2SMEM pool, kernel_pool.cu:39-48): columns of
+// n2 words and rows of n1 words, transformed in shared memory; the result of
+// the forward transform is in fully bit-reversed order, like the radix-2
+// kernels, so all plans share the 4-step twiddle tables.
 //
 // row_square_r16: the first pass reads HBM directly (with the 4-step twiddle)
 // and the last inverse pass writes HBM directly; the last forward pass, the
@@ -27,144 +16,19 @@
 #include "carry.cuh"
 #include "lnt_internal.h"
 #include "ntt_core.cuh"
+#include "smem_passes.cuh"
 
 namespace lnt {
 
 namespace {
 
-__device__ __forceinline__ int sw(int i) { return i + (i >> 4); }
-__host__ __device__ constexpr int padded(int L) { return L + L / 16; }
-
-struct Passes {
-  int m;          // number of passes
-  int radix[6];   // r_0 (largest stride) ... r_{m-1} (contiguous)
-};
-
-// Largest pass radix.  8 (three radix-2 stages per pass) keeps a task's values,
-// twiddles and addresses within the 64 registers that four row CTAs (two column
-// CTAs) per SM allow; 16 needs one twiddle stage less per direction but spills
-// (measured at n = 2^23: 561 us per squaring with 8, 574 with 16).
-#ifndef LNT_MAX_RADIX_LOG2
-#define LNT_MAX_RADIX_LOG2 3
-#endif
-constexpr int kMaxRadix = 1 << LNT_MAX_RADIX_LOG2;
-
-Passes make_passes(int log2L) {
-  constexpr int b = LNT_MAX_RADIX_LOG2;
-  Passes p{};
-  int first = log2L % b;
-  int rest = log2L - first;
-  if (first == 0) {
-    first = b;
-    rest -= b;
-  }
-  p.radix[p.m++] = 1 << first;
-  for (int k = 0; k < rest / b; ++k) p.radix[p.m++] = 1 << b;
-  return p;
-}
-
-// ---- one task: R elements of one block, forward or inverse ----------------
-
-// The R twiddles of one task, a 16-byte aligned run of the pass table: read as
-// R/2 vector loads from one base address.
-#ifndef LNT_TW_UNROLL
-#define LNT_TW_UNROLL 8  // twiddle vectors loaded per unrolled step (register pressure)
-#endif
-constexpr int kTwUnroll = LNT_TW_UNROLL;
-template <int R>
-__device__ __forceinline__ void mul_task_twiddles(uint64_t (&v)[R], const uint64_t* tw) {
-  const ulonglong2* w2 = reinterpret_cast<const ulonglong2*>(tw);
-#pragma unroll kTwUnroll
-  for (int k = 0; k < R / 2; ++k) {
-    const ulonglong2 u = __ldg(w2 + k);
-    v[2 * k] = gl::mul(v[2 * k], u.x);
-    v[2 * k + 1] = gl::mul(v[2 * k + 1], u.y);
-  }
-}
-
-// forward: DIF, then omega_span^(t k) (tw: this task's twiddles; unused when q == 1)
-template <int R>
-__device__ __forceinline__ void task_dif(uint64_t* base, int off, int q, const uint64_t* tw) {
-  uint64_t v[R];
-#pragma unroll
-  for (int d = 0; d < R; ++d) v[d] = base[sw(off + q * d)];
-  dif<R>(v);
-  if (q > 1) mul_task_twiddles<R>(v, tw);
-#pragma unroll
-  for (int r = 0; r < R; ++r) base[sw(off + q * r)] = v[r];
-}
-
-// inverse: omega_span^-(t k), then DIT
-template <int R>
-__device__ __forceinline__ void task_dit(uint64_t* base, int off, int q, const uint64_t* itw) {
-  uint64_t v[R];
-#pragma unroll
-  for (int r = 0; r < R; ++r) v[r] = base[sw(off + q * r)];
-  if (q > 1) mul_task_twiddles<R>(v, itw);
-  dit_inv<R>(v);
-#pragma unroll
-  for (int d = 0; d < R; ++d) base[sw(off + q * d)] = v[d];
-}
-
-// Offset of pass j's twiddles in a pass table (the spans of the passes before it).
-__device__ __forceinline__ int pass_table_offset(const Passes& P, int L, int j) {
-  int off = 0, span = L;
-  for (int i = 0; i < j; ++i) {
-    off += span;
-    span /= P.radix[i];
-  }
-  return off;
-}
-
-// last forward pass, pointwise square and first inverse pass (contiguous blocks)
-template <int R>
-__device__ __forceinline__ void task_square(uint64_t* base, int off) {
-  uint64_t v[R];
-#pragma unroll
-  for (int d = 0; d < R; ++d) v[d] = base[sw(off + d)];
-  dif<R>(v);
-#pragma unroll
-  for (int d = 0; d < R; ++d) v[d] = gl::sqr(v[d]);
-  dit_inv<R>(v);
-#pragma unroll
-  for (int d = 0; d < R; ++d) base[sw(off + d)] = v[d];
-}
-
-// A pass over `ntrans` transforms of length L; transform g lives at sm + g * ld.
-// tw: this pass's part of the pass table.
-template <int R, int Mode>  // Mode 0: DIF, 1: DIT, 2: square
-__device__ void pass(uint64_t* sm, int ld, int ntrans, int L, int span, const uint64_t* tw) {
-  // all sizes are powers of two: index arithmetic by shifts and masks
-  const int q = span / R, per = L / R;
-  const int lq = __ffs(q) - 1, lper = __ffs(per) - 1;
-  const int total = ntrans * per;
-  for (int task = threadIdx.x; task < total; task += blockDim.x) {
-    const int g = task >> lper, k = task & (per - 1);
-    const int b = k >> lq, t = k & (q - 1);
-    uint64_t* base = sm + g * ld;
-    if constexpr (Mode == 0)
-      task_dif<R>(base, b * span + t, q, tw + t * R);
-    else if constexpr (Mode == 1)
-      task_dit<R>(base, b * span + t, q, tw + t * R);
-    else
-      task_square<R>(base, b * span);
-  }
-}
-
-template <int Mode>
-__device__ __forceinline__ void pass_r(int R, uint64_t* sm, int ld, int ntrans, int L, int span,
-                                       const uint64_t* tw) {
-  switch (R) {
-    case 2: pass<2, Mode>(sm, ld, ntrans, L, span, tw); break;
-    case 4: pass<4, Mode>(sm, ld, ntrans, L, span, tw); break;
-    case 8: pass<8, Mode>(sm, ld, ntrans, L, span, tw); break;
-    default: pass<kMaxRadix, Mode>(sm, ld, ntrans, L, span, tw); break;
-  }
-}
+using namespace smem;
 
 // ------------------------------------------------------------------ rows ----
 
-constexpr int kRowThreads = 256;
+// 256 threads per row of up to 4096 words (four CTAs per SM); longer rows hold
+// one or two CTAs per SM, so their CTAs are wider to keep 32 warps per SM.
+constexpr int row_threads_for(int L) { return L <= 4096 ? 256 : (L == 8192 ? 512 : 1024); }
 #ifndef LNT_ROW_MIN_BLOCKS
 #define LNT_ROW_MIN_BLOCKS 4  // CTAs per SM the row kernel is compiled for (registers)
 #endif
@@ -249,7 +113,8 @@ __device__ __forceinline__ void row_pass_r(int R, uint64_t* sm, int ld, int rows
   }
 }
 
-__global__ void __launch_bounds__(kRowThreads, LNT_ROW_MIN_BLOCKS) row_square_r16(const TwoPassDesc* __restrict__ Ds, Passes P, int rows) {
+template <int TH>
+__global__ void __launch_bounds__(TH, TH == 256 ? LNT_ROW_MIN_BLOCKS : 1024 / TH) row_square_r16(const TwoPassDesc* __restrict__ Ds, Passes P, int rows) {
   extern __shared__ __align__(16) uint64_t sm[];
   const TwoPassDesc& D = Ds[blockIdx.y];
   const int L = (int)D.n1, ld = padded(L);
@@ -351,8 +216,8 @@ __device__ __forceinline__ void load_widths(const uint8_t* src, unsigned (&out)[
   }
 }
 
-template <int T>
-__global__ void __launch_bounds__(col_threads<T>(), col_min_blocks<T>()) col_forward_r16(const TwoPassDesc* __restrict__ Ds,
+template <int T, int TH>
+__global__ void __launch_bounds__(TH, TH == col_threads<T>() ? col_min_blocks<T>() : 1) col_forward_r16(const TwoPassDesc* __restrict__ Ds,
                                                                       Passes P, int apply_carries) {
   extern __shared__ __align__(16) uint64_t sm[];
   const TwoPassDesc& D = Ds[blockIdx.y];
@@ -401,8 +266,8 @@ __global__ void __launch_bounds__(col_threads<T>(), col_min_blocks<T>()) col_for
   if (status) atomicOr(D.status, status);
 }
 
-template <int T>
-__global__ void __launch_bounds__(col_threads<T>(), col_min_blocks<T>()) col_inverse_r16(const TwoPassDesc* __restrict__ Ds,
+template <int T, int TH>
+__global__ void __launch_bounds__(TH, TH == col_threads<T>() ? col_min_blocks<T>() : 1) col_inverse_r16(const TwoPassDesc* __restrict__ Ds,
                                                                       Passes P, int unsigned_mode) {
   extern __shared__ __align__(16) uint64_t sm[];
   const TwoPassDesc& D = Ds[blockIdx.y];
@@ -496,49 +361,63 @@ uint32_t r16_run_words_needed(uint32_t exponent, uint32_t log2n) {
   return (log2n + wmax + wmin - 2) / (wmin - 1) + 1;
 }
 
-cudaError_t launch_row_square_r16(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
-                                  cudaStream_t s) {
+template <int TH>
+cudaError_t row_square_t(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count, cudaStream_t s) {
   const int L = (int)d.n1, rows = row_rows_per_cta(L, (int)d.n2);
   const size_t smem = (size_t)rows * padded(L) * 8;
-  cudaError_t e = ensure_smem(row_square_r16, smem);
+  cudaError_t e = ensure_smem(row_square_r16<TH>, smem);
   if (e != cudaSuccess) return e;
-  row_square_r16<<<dim3(d.n2 / rows, count), kRowThreads, smem, s>>>(dd, make_passes((int)d.log2n1),
-                                                                     rows);
+  row_square_r16<TH><<<dim3(d.n2 / rows, count), TH, smem, s>>>(dd, make_passes((int)d.log2n1), rows);
   return cudaGetLastError();
 }
 
+cudaError_t launch_row_square_r16(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
+                                  cudaStream_t s) {
+  switch (row_threads_for((int)d.n1)) {
+    case 256: return row_square_t<256>(d, dd, count, s);
+    case 512: return row_square_t<512>(d, dd, count, s);
+    default: return row_square_t<1024>(d, dd, count, s);
+  }
+}
+
+// Columns of 4096 words hold one CTA per SM: 1024 threads instead of 128 per column.
 template <int T>
+constexpr int col_wide_threads() { return 1024; }
+
+template <int T, int TH>
 cudaError_t col_forward_t(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count, bool apply,
                           cudaStream_t s) {
   const size_t smem = (size_t)T * col_ld((int)d.n2, T) * 8;
-  cudaError_t e = ensure_smem(col_forward_r16<T>, smem);
+  cudaError_t e = ensure_smem(col_forward_r16<T, TH>, smem);
   if (e != cudaSuccess) return e;
-  col_forward_r16<T><<<dim3(d.ntiles, count), col_threads<T>(), smem, s>>>(
-      dd, make_passes((int)d.log2n2), apply ? 1 : 0);
+  col_forward_r16<T, TH><<<dim3(d.ntiles, count), TH, smem, s>>>(dd, make_passes((int)d.log2n2),
+                                                                  apply ? 1 : 0);
   return cudaGetLastError();
 }
 
-template <int T>
+template <int T, int TH>
 cudaError_t col_inverse_t(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
                           bool unsigned_mode, cudaStream_t s) {
   const size_t smem = (size_t)T * col_ld((int)d.n2, T) * 8;
-  cudaError_t e = ensure_smem(col_inverse_r16<T>, smem);
+  cudaError_t e = ensure_smem(col_inverse_r16<T, TH>, smem);
   if (e != cudaSuccess) return e;
-  col_inverse_r16<T><<<dim3(d.ntiles, count), col_threads<T>(), smem, s>>>(
-      dd, make_passes((int)d.log2n2), unsigned_mode ? 1 : 0);
+  col_inverse_r16<T, TH><<<dim3(d.ntiles, count), TH, smem, s>>>(dd, make_passes((int)d.log2n2),
+                                                                  unsigned_mode ? 1 : 0);
   return cudaGetLastError();
 }
 
 cudaError_t launch_col_forward_r16(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
                                    bool apply, cudaStream_t s) {
-  return d.tile == 4 ? col_forward_t<4>(d, dd, count, apply, s)
-                     : col_forward_t<8>(d, dd, count, apply, s);
+  if (d.tile == 8) return col_forward_t<8, col_threads<8>()>(d, dd, count, apply, s);
+  if (d.n2 >= 4096) return col_forward_t<4, col_wide_threads<4>()>(d, dd, count, apply, s);
+  return col_forward_t<4, col_threads<4>()>(d, dd, count, apply, s);
 }
 
 cudaError_t launch_col_inverse_r16(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
                                    bool unsigned_mode, cudaStream_t s) {
-  return d.tile == 4 ? col_inverse_t<4>(d, dd, count, unsigned_mode, s)
-                     : col_inverse_t<8>(d, dd, count, unsigned_mode, s);
+  if (d.tile == 8) return col_inverse_t<8, col_threads<8>()>(d, dd, count, unsigned_mode, s);
+  if (d.n2 >= 4096) return col_inverse_t<4, col_wide_threads<4>()>(d, dd, count, unsigned_mode, s);
+  return col_inverse_t<4, col_threads<4>()>(d, dd, count, unsigned_mode, s);
 }
 
 }  // namespace lnt
