@@ -210,6 +210,40 @@ GL_HD uint64_t mul_pow2(uint64_t x, unsigned s) {
   return negate ? neg(r) : r;
 }
 
+// d * w for a digit |d| < 2^32 (a balanced or non-negative residue word) and a
+// field element w: a 32 x 64-bit product (96 bits, so the reduction has no
+// 2^96 term), then the sign.  Equals mul(from_signed(d), w).
+GL_HD uint64_t mul_digit(int64_t d, uint64_t w) {
+  const bool negative = d < 0;
+  const uint32_t a = (uint32_t)(negative ? -d : d);
+#if defined(__CUDA_ARCH__)
+  uint32_t t0, t1;
+  asm("{\n\t"
+      ".reg .u32 r2, u0, u1, c, m;\n\t"
+      "mul.lo.u32     %0, %2, %3;\n\t"
+      "mul.hi.u32     %1, %2, %3;\n\t"
+      "mad.lo.cc.u32  %1, %2, %4, %1;\n\t"
+      "madc.hi.u32    r2, %2, %4, 0;\n\t"
+      // (t1:t0) + r2 (2^32 - 1): plus (r2 - [r2 != 0]) : (0 - r2)
+      "sub.cc.u32     u0, 0, r2;\n\t"
+      "subc.u32       u1, r2, 0;\n\t"
+      "add.cc.u32     %0, %0, u0;\n\t"
+      "addc.cc.u32    %1, %1, u1;\n\t"
+      "addc.u32       c, 0, 0;\n\t"
+      "neg.s32        m, c;\n\t"
+      "add.cc.u32     %0, %0, m;\n\t"
+      "addc.u32       %1, %1, 0;\n\t"
+      "}"
+      : "=r"(t0), "=r"(t1)
+      : "r"(a), "r"((uint32_t)w), "r"((uint32_t)(w >> 32)));
+  uint64_t r = ((uint64_t)t1 << 32) | t0;
+  r = r >= P ? r - P : r;
+#else
+  const uint64_t r = reduce128((uint64_t)a * w, mulhi((uint64_t)a, w));
+#endif
+  return negative ? neg(r) : r;
+}
+
 // Balanced digit d (|d| < 2^62) as a field element.
 GL_HD uint64_t from_signed(int64_t d) { return d >= 0 ? (uint64_t)d : (uint64_t)d + P; }
 

@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(TH, TH == col_threads<T>() ? col_min_blocks<T>
           carry = 0;
         }
       }
-      v = gl::mul(gl::from_signed(d), w[c]);
+      v = gl::mul_digit(d, w[c]);
     }
   }
   __syncthreads();

@@ -58,7 +58,7 @@ __global__ void __launch_bounds__(kMaxThreads) resident_square_loop(const Reside
   for (uint64_t it = 0; it < D.iterations; ++it) {
     const bool um = D.unsigned_first && it == 0;
     // weight the digits (balanced digits become field elements)
-    for (uint32_t j = tid; j < n; j += bd) s[sw(j)] = gl::mul(gl::from_signed((int64_t)s[sw(j)]), w[j]);
+    for (uint32_t j = tid; j < n; j += bd) s[sw(j)] = gl::mul_digit((int64_t)s[sw(j)], w[j]);
     __syncthreads();
     // forward passes, the last one fused with the square and the first inverse pass
     int span = (int)n;

@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(kThreads) col_forward(TwoPassDesc D, int apply
   for (uint32_t idx = threadIdx.x; idx < T * n2; idx += blockDim.x) {
     const uint32_t r = idx / T, c = idx % T;
     uint64_t& v = sm[(size_t)c * ld + r];
-    v = gl::mul(gl::from_signed((int64_t)v), D.w[(size_t)r * n1 + c0 + c]);
+    v = gl::mul_digit((int64_t)v, D.w[(size_t)r * n1 + c0 + c]);
   }
   __syncthreads();
   columns_forward(sm, ld, T, n2, D.log2n2, D.rt2);

@@ -40,6 +40,16 @@ int main() {
   CHECK(gl::pow(554, (P - 1) / 64) == 8, "omega_64 != 8");
   CHECK(gl::pow(gl::pow(7, (P - 1) / 192 * 5), 1) == 2, "7^(5(p-1)/192) != 2");
   for (uint64_t a : vals) if (a) CHECK(gl::mul(a, gl::inv(a)) == 1, "inv %llx", (unsigned long long)a);
+  // digit x weight: |d| < 2^32 times a field element, against the general product
+  {
+    std::vector<int64_t> ds = {0, 1, -1, 2, -2, (1ll << 31) - 1, -(1ll << 31), (1ll << 32) - 1,
+                               -((1ll << 32) - 1), 65535, -65536};
+    for (int i = 0; i < 2000; ++i) ds.push_back((int64_t)(rng() >> 31) - (int64_t)(1ull << 32));
+    for (int64_t d : ds)
+      for (size_t k = 0; k < vals.size(); k += 7)
+        CHECK(gl::mul_digit(d, vals[k]) == gl::mul(gl::from_signed(d), vals[k]), "mul_digit %lld %llx",
+              (long long)d, (unsigned long long)vals[k]);
+  }
   // signed views
   for (int64_t d : {0ll, 1ll, -1ll, 12345ll, -12345ll, (1ll << 40), -(1ll << 40)})
     CHECK(gl::to_signed(gl::from_signed(d)) == d, "signed round trip %lld", (long long)d);
