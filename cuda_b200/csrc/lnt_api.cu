@@ -43,6 +43,7 @@ struct lnt_test {
   uint64_t *wt = nullptr, *uwt = nullptr;
   uint8_t* widt = nullptr;
   int64_t* carry = nullptr;
+  uint32_t* fuse = nullptr;  // carry-fused column kernel: ticket, epoch, tile flags
   // canonical readout
   uint64_t* canon = nullptr;
   int64_t* blk_carry = nullptr;
@@ -102,7 +103,7 @@ cudaError_t dalloc(T** p, size_t count) {
 void free_all(lnt_test* t) {
   void* ptrs[] = {t->x, t->w, t->uw, t->widths, t->status, t->rt, t->irt, t->rdesc, t->tdesc,
                   t->twf, t->twi, t->rt1, t->irt1, t->rt2, t->irt2, t->itw1, t->iitw1,
-                  t->itw2, t->iitw2, t->wt, t->uwt, t->widt, t->carry, t->canon,
+                  t->itw2, t->iitw2, t->wt, t->uwt, t->widt, t->carry, t->fuse, t->canon,
                   t->blk_carry, t->blk_fn, t->blk_cin, t->cflags};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -186,6 +187,7 @@ lnt::TwoPassDesc twopass_desc(const lnt_test* t) {
   d.irt1 = t->irt1;
   d.rt2 = t->rt2;
   d.irt2 = t->irt2;
+  d.fuse = t->fuse;
   d.itw1 = t->itw1;
   d.iitw1 = t->iitw1;
   d.itw2 = t->itw2;
@@ -254,6 +256,8 @@ int check_status(lnt_test* t) {
   LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
   if (t->h_pinned[0] & lnt::kStatusCarryOverflow)
     return fail(LNT_ERR_NUMERIC, "carry exceeded the balanced-digit headroom");
+  if (t->h_pinned[0] & lnt::kStatusFuseTimeout)
+    return fail(LNT_ERR_CUDA, "a carry-fused column CTA timed out waiting for its neighbour");
   return LNT_OK;
 }
 
@@ -366,8 +370,10 @@ struct LaunchTimer {
 // Squarings per captured graph: launch overhead amortised over 3 x 16 kernels.
 constexpr uint64_t kGraphSquarings = 16;
 
-// Capture kGraphSquarings steady-state squarings of a pass-kernel test on its
-// stream.  On any failure the test keeps plain launches (graph_failed).
+// Capture kGraphSquarings steady-state squarings on the test's stream: each a
+// fused column launch (the inverse half of one squaring and the forward half of
+// the next) and a row launch, or, without fusion, the three launches of a
+// squaring.  On any failure the test keeps plain launches (graph_failed).
 void capture_graph(lnt_test* t, const lnt::TwoPassDesc& d) {
   cudaGraph_t g = nullptr;
   if (cudaStreamBeginCapture(t->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
@@ -377,9 +383,12 @@ void capture_graph(lnt_test* t, const lnt::TwoPassDesc& d) {
   }
   bool ok = true;
   for (uint64_t k = 0; k < kGraphSquarings && ok; ++k)
-    ok = lnt::launch_col_forward_r16(d, t->tdesc, 1, true, t->stream) == cudaSuccess &&
-         lnt::launch_row_square_r16(d, t->tdesc, 1, t->stream) == cudaSuccess &&
-         lnt::launch_col_inverse_r16(d, t->tdesc, 1, false, t->stream) == cudaSuccess;
+    ok = t->plan.fused
+             ? lnt::launch_col_fused_r16(d, t->tdesc, 1, t->stream) == cudaSuccess &&
+                   lnt::launch_row_square_r16(d, t->tdesc, 1, t->stream) == cudaSuccess
+             : lnt::launch_col_forward_r16(d, t->tdesc, 1, true, t->stream) == cudaSuccess &&
+                   lnt::launch_row_square_r16(d, t->tdesc, 1, t->stream) == cudaSuccess &&
+                   lnt::launch_col_inverse_r16(d, t->tdesc, 1, false, t->stream) == cudaSuccess;
   const cudaError_t e = cudaStreamEndCapture(t->stream, &g);
   if (ok && e == cudaSuccess && g && cudaGraphInstantiate(&t->graph, g, 0) != cudaSuccess) t->graph = nullptr;
   if (g) cudaGraphDestroy(g);
@@ -409,31 +418,54 @@ int queue_iterations(lnt_test* t, uint64_t iterations, LaunchTimer* timer) {
     LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
   } else {
     lnt::TwoPassDesc d = twopass_desc(t);
-    uint64_t i = 0;
-    // steady state (carries pending, signed outputs): whole chunks replay a graph
-    auto steady = [&]() { return t->pending_carries && !t->canonical_input; };
-    for (; i < iterations; ++i) {
-      if (t->plan.fast && !timer && steady() && iterations - i >= kGraphSquarings && !t->graph_failed) {
-        if (!t->graph) capture_graph(t, d);
-        if (t->graph) {
-          for (; iterations - i >= kGraphSquarings; i += kGraphSquarings)
-            LNT_CUDA(cudaGraphLaunch(t->graph, t->stream), "graph launch");
-          if (i == iterations) break;
-        }
-      }
-      if (t->plan.fast) {
+    if (t->plan.fast) {
+      uint64_t left = iterations;
+      if (t->canonical_input) {
+        // the first squaring of non-negative digits reads its outputs unsigned
         LNT_LAUNCH(lnt::launch_col_forward_r16(d, t->tdesc, 1, t->pending_carries, t->stream),
                    "col_forward");
         LNT_LAUNCH(lnt::launch_row_square_r16(d, t->tdesc, 1, t->stream), "row_square");
-        LNT_LAUNCH(lnt::launch_col_inverse_r16(d, t->tdesc, 1, t->canonical_input, t->stream),
-                   "col_inverse");
-      } else {
+        LNT_LAUNCH(lnt::launch_col_inverse_r16(d, t->tdesc, 1, true, t->stream), "col_inverse");
+        t->pending_carries = true;
+        t->canonical_input = false;
+        --left;
+      }
+      if (left && t->plan.fused) {
+        // col_forward, then (row, fused col_inverse + col_forward) x (left - 1),
+        // row, col_inverse: between calls the state stays digits + carries
+        LNT_LAUNCH(lnt::launch_col_forward_r16(d, t->tdesc, 1, true, t->stream), "col_forward");
+        LNT_LAUNCH(lnt::launch_row_square_r16(d, t->tdesc, 1, t->stream), "row_square");
+        uint64_t mid = left - 1;
+        if (!timer && mid >= kGraphSquarings && !t->graph_failed && !t->graph) capture_graph(t, d);
+        if (!timer && t->graph)
+          for (; mid >= kGraphSquarings; mid -= kGraphSquarings)
+            LNT_CUDA(cudaGraphLaunch(t->graph, t->stream), "graph launch");
+        for (; mid > 0; --mid) {
+          LNT_LAUNCH(lnt::launch_col_fused_r16(d, t->tdesc, 1, t->stream), "col_fused");
+          LNT_LAUNCH(lnt::launch_row_square_r16(d, t->tdesc, 1, t->stream), "row_square");
+        }
+        LNT_LAUNCH(lnt::launch_col_inverse_r16(d, t->tdesc, 1, false, t->stream), "col_inverse");
+      } else if (left) {
+        // three launches per squaring; whole graphs of kGraphSquarings squarings
+        if (!timer && left >= kGraphSquarings && !t->graph_failed && !t->graph) capture_graph(t, d);
+        if (!timer && t->graph)
+          for (; left >= kGraphSquarings; left -= kGraphSquarings)
+            LNT_CUDA(cudaGraphLaunch(t->graph, t->stream), "graph launch");
+        for (; left > 0; --left) {
+          LNT_LAUNCH(lnt::launch_col_forward_r16(d, t->tdesc, 1, true, t->stream), "col_forward");
+          LNT_LAUNCH(lnt::launch_row_square_r16(d, t->tdesc, 1, t->stream), "row_square");
+          LNT_LAUNCH(lnt::launch_col_inverse_r16(d, t->tdesc, 1, false, t->stream), "col_inverse");
+        }
+      }
+      t->pending_carries = true;
+    } else {
+      for (uint64_t i = 0; i < iterations; ++i) {
         LNT_LAUNCH(lnt::launch_col_forward(d, t->pending_carries, t->stream), "col_forward");
         LNT_LAUNCH(lnt::launch_row_square(d, t->stream), "row_square");
         LNT_LAUNCH(lnt::launch_col_inverse(d, t->canonical_input, t->stream), "col_inverse");
+        t->pending_carries = true;
+        t->canonical_input = false;
       }
-      t->pending_carries = true;
-      t->canonical_input = false;
     }
   }
   t->canonical_input = false;
@@ -491,7 +523,8 @@ uint64_t test_device_bytes(uint32_t n) {
     b += 8ull * n + sizeof(ResidentDesc);  // root tables
   } else {
     // carry buffer: one word per run, at most n / 4 runs (the narrowest tile)
-    b += 16ull * n + 8ull * (plan.n1 + plan.n2) + 2ull * n + sizeof(TwoPassDesc);
+    b += 16ull * n + 8ull * (plan.n1 + plan.n2) + 2ull * n + sizeof(TwoPassDesc) +
+         4ull * (plan.n1 + 2);  // fused-kernel flags
     if (plan.fast) b += 16ull * (plan.n1 + plan.n2) + 17ull * n;  // inner twiddles, tile-major tables
   }
   return b;
@@ -597,7 +630,9 @@ int lnt_create_with_plan(uint32_t exponent, uint32_t n, int prp, int device,
         return bail(cuda_fail(e, "tile-major tables"));
     }
     if ((e = dalloc(&t->twf, n)) || (e = dalloc(&t->twi, n)) ||
-        (e = dalloc(&t->carry, (size_t)plan.ntiles * plan.n2)))
+        (e = dalloc(&t->carry, (size_t)plan.ntiles * plan.n2)) ||
+        (e = dalloc(&t->fuse, (size_t)plan.ntiles + 2)) ||
+        (e = cudaMemset(t->fuse, 0, ((size_t)plan.ntiles + 2) * 4)))
       return bail(cuda_fail(e, "allocate twiddles"));
     if ((e = lnt::launch_twiddles(plan.n1, plan.n2, plan.log2n2, t->twf, t->twi, t->stream)))
       return bail(cuda_fail(e, "twiddles"));

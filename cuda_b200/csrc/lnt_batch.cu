@@ -64,6 +64,7 @@ constexpr uint64_t kGraphChunk = 8;  // squarings per captured graph
 
 struct Group {
   uint32_t n = 0;
+  bool fused = false;  // the plan's steady squarings use the carry-fused column kernel
   std::vector<size_t> members;  // indices into active
   lnt::TwoPassDesc geometry{};
   lnt::TwoPassDesc* d_descs = nullptr;
@@ -150,9 +151,20 @@ int launch_groups(lnt_batch* b, uint64_t k) {
     Group& g = kv.second;
     const uint32_t cnt = (uint32_t)g.members.size();
     BCUDA(cudaStreamWaitEvent(g.stream, b->fork, 0), "fork wait");
-    for (uint64_t it = 0; it < k; ++it) {
+    if (!g.fused) {
+      for (uint64_t it = 0; it < k; ++it) {
+        BCUDA(lnt::launch_col_forward_r16(g.geometry, g.d_descs, cnt, true, g.stream), "col_forward");
+        BCUDA(lnt::launch_row_square_r16(g.geometry, g.d_descs, cnt, g.stream), "row_square");
+        BCUDA(lnt::launch_col_inverse_r16(g.geometry, g.d_descs, cnt, false, g.stream), "col_inverse");
+      }
+    } else if (k > 0) {
+      // col_forward, row, (fused col_inverse + col_forward, row) x (k - 1), col_inverse
       BCUDA(lnt::launch_col_forward_r16(g.geometry, g.d_descs, cnt, true, g.stream), "col_forward");
       BCUDA(lnt::launch_row_square_r16(g.geometry, g.d_descs, cnt, g.stream), "row_square");
+      for (uint64_t it = 1; it < k; ++it) {
+        BCUDA(lnt::launch_col_fused_r16(g.geometry, g.d_descs, cnt, g.stream), "col_fused");
+        BCUDA(lnt::launch_row_square_r16(g.geometry, g.d_descs, cnt, g.stream), "row_square");
+      }
       BCUDA(lnt::launch_col_inverse_r16(g.geometry, g.d_descs, cnt, false, g.stream), "col_inverse");
     }
     BCUDA(cudaEventRecord(g.join, g.stream), "join");
@@ -199,6 +211,7 @@ int rebuild(lnt_batch* b) {
       // one launch serves tests of identical geometry: same length and tile width
       Group& g = b->groups[GroupKey{p.n, p.log2n2, p.tile}];
       g.n = p.n;
+      g.fused = p.fused;
       g.members.push_back(i);
     } else {
       b->singles.push_back(i);

@@ -12,6 +12,7 @@ namespace lnt {
 enum : uint32_t {
   kStatusCarryOverflow = 1u << 0,  // a run absorbed a carry above kAbsorbLimit
   kStatusCanonFallback = 1u << 1,  // canonical readout needs the host fallback
+  kStatusFuseTimeout = 1u << 2,    // a carry-fused column CTA gave up waiting for its neighbour
 };
 
 // ---------------------------------------------------------------- plans ----
@@ -28,7 +29,12 @@ struct Plan {
   uint32_t n1 = 0, n2 = 0, log2n1 = 0, log2n2 = 0;
   uint32_t tile = 0;    // columns per column-pass CTA = words per carry run
   uint32_t ntiles = 0;  // n1 / tile
-  bool fast = false;    // radix-16 pass kernels (lnt_radix16.cu) instead of radix-2
+  bool fast = false;    // register-pass kernels (lnt_radix16.cu) instead of radix-2
+  // steady squarings use the carry-fused column kernel (col_inverse of one
+  // squaring + col_forward of the next): from 2^19 words, where its tiles fill
+  // the GPU (at n = 2^23: 297 us for the pair that takes 308 us as two
+  // launches); below, where a squaring is latency-bound, two plain launches win
+  bool fused = false;
   std::string name;
 };
 
@@ -99,6 +105,8 @@ struct TwoPassDesc {
   const uint64_t* uwt;
   const uint8_t* widt;
   uint32_t* status;
+  // carry-fused column kernel: [0] ticket, [1] epoch, [2 + t] flag of tile t (zeroed at creation)
+  uint32_t* fuse;
   uint32_t n1, n2, log2n1, log2n2, tile, ntiles;
   uint32_t prp;
 };
@@ -123,6 +131,10 @@ cudaError_t launch_row_square_r16(const TwoPassDesc& d, const TwoPassDesc* dd, u
                                   cudaStream_t s);
 cudaError_t launch_col_inverse_r16(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
                                    bool unsigned_mode, cudaStream_t s);
+// col_inverse of one squaring and col_forward of the next (steady state: carries
+// pending, signed outputs) in one launch
+cudaError_t launch_col_fused_r16(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
+                                 cudaStream_t s);
 
 // ------------------------------------------------------------- tables ----
 cudaError_t launch_weights(uint32_t exponent, uint32_t n, uint64_t* w, uint64_t* uw,

@@ -162,6 +162,7 @@ bool make_plan(uint32_t n, uint32_t exponent, const PlanOptions* opt, Plan& plan
   plan.n2 = 1u << l2;
   plan.tile = tile;
   plan.ntiles = plan.n1 / plan.tile;
+  plan.fused = plan.fast && plan.log2n >= 19;
   name_plan(plan);
   return true;
 }

@@ -216,17 +216,16 @@ __device__ __forceinline__ void load_widths(const uint8_t* src, unsigned (&out)[
   }
 }
 
-template <int T, int TH>
-__global__ void __launch_bounds__(TH, TH == col_threads<T>() ? col_min_blocks<T>() : 1) col_forward_r16(const TwoPassDesc* __restrict__ Ds,
-                                                                      Passes P, int apply_carries) {
-  extern __shared__ __align__(16) uint64_t sm[];
-  const TwoPassDesc& D = Ds[blockIdx.y];
-  const int L = (int)D.n2, ld = col_ld(L, T);
-  const uint32_t n1 = D.n1, t0 = blockIdx.x, c0 = t0 * T;
-  uint32_t status = 0;
+// ---- column tile bodies: tile t0 (T columns x L rows) staged in shared memory
 
-  tile_load(sm, ld, D.x, L, T, n1, c0);
-  __syncthreads();
+// Carry-in from the run before each row's run, weight, forward column passes,
+// store.  The tile's digits are in `sm`.  `cg_carries`: read the carries from L2
+// (written by another CTA of the same launch).
+template <int T>
+__device__ __forceinline__ void forward_tile(const TwoPassDesc& D, const Passes& P, uint64_t* sm,
+                                             int ld, uint32_t t0, bool apply_carries, bool cg_carries,
+                                             uint32_t& status) {
+  const int L = (int)D.n2;
   // per row: carry from the previous run, then weight (balanced digit -> field)
   for (int r = threadIdx.x; r < L; r += blockDim.x) {
     const size_t run = (size_t)t0 * L + r;
@@ -235,7 +234,10 @@ __global__ void __launch_bounds__(TH, TH == col_threads<T>() ? col_min_blocks<T>
     load_run<T>(D.wt + run * T, w);
     load_widths<T>(D.widt + run * T, wd);
     int64_t carry = 0;
-    if (apply_carries) carry = D.carry[t0 > 0 ? run - L : (size_t)(D.ntiles - 1) * L + (r ? r - 1 : L - 1)];
+    if (apply_carries) {
+      const int64_t* src = D.carry + (t0 > 0 ? run - L : (size_t)(D.ntiles - 1) * L + (r ? r - 1 : L - 1));
+      carry = cg_carries ? __ldcg(src) : *src;
+    }
 #pragma unroll
     for (int c = 0; c < T; ++c) {
       uint64_t& v = sm[c * ld + sw(r)];
@@ -262,27 +264,22 @@ __global__ void __launch_bounds__(TH, TH == col_threads<T>() ? col_min_blocks<T>
     span /= P.radix[j];
     __syncthreads();
   }
-  tile_store(sm, ld, D.x, L, T, n1, c0);
-  if (status) atomicOr(D.status, status);
+  tile_store(sm, ld, D.x, L, T, D.n1, t0 * T);
 }
 
-template <int T, int TH>
-__global__ void __launch_bounds__(TH, TH == col_threads<T>() ? col_min_blocks<T>() : 1) col_inverse_r16(const TwoPassDesc* __restrict__ Ds,
-                                                                      Passes P, int unsigned_mode) {
-  extern __shared__ __align__(16) uint64_t sm[];
-  const TwoPassDesc& D = Ds[blockIdx.y];
-  const int L = (int)D.n2, ld = col_ld(L, T);
-  const uint32_t n1 = D.n1, t0 = blockIdx.x, c0 = t0 * T;
-
-  tile_load(sm, ld, D.x, L, T, n1, c0);
-  __syncthreads();
+// Inverse column passes, unweight, carry each row's run of T words to balanced
+// digits (minus two in the run of word 0), store the runs' outgoing carries.
+// The tile's transform is in `sm`; its digits are left there.
+template <int T>
+__device__ __forceinline__ void inverse_tile(const TwoPassDesc& D, const Passes& P, uint64_t* sm,
+                                             int ld, uint32_t t0, bool unsigned_mode) {
+  const int L = (int)D.n2;
   int span = 1;
   for (int j = P.m - 1; j >= 0; --j) {
     span *= P.radix[j];
     pass_r<1>(P.radix[j], sm, ld, T, L, span, D.iitw2 + pass_table_offset(P, L, j));
     __syncthreads();
   }
-  // per row: unweight, carry the run of T words to balanced digits, minus two
   for (int r = threadIdx.x; r < L; r += blockDim.x) {
     const size_t run = (size_t)t0 * L + r;
     uint64_t uw[T];
@@ -294,14 +291,135 @@ __global__ void __launch_bounds__(TH, TH == col_threads<T>() ? col_min_blocks<T>
     for (int c = 0; c < T; ++c) {
       uint64_t& v = sm[c * ld + sw(r)];
       int64_t hi, lo, q;
-      split_output(gl::mul(v, uw[c]), unsigned_mode != 0, wd[c], hi, lo);
+      split_output(gl::mul(v, uw[c]), unsigned_mode, wd[c], hi, lo);
       v = (uint64_t)balance(lo + carry, wd[c], q);
       carry = hi + q;
     }
     D.carry[run] = carry;
   }
   __syncthreads();
-  tile_store(sm, ld, D.x, L, T, n1, c0);
+}
+
+template <int T, int TH>
+__global__ void __launch_bounds__(TH, TH == col_threads<T>() ? col_min_blocks<T>() : 1) col_forward_r16(
+    const TwoPassDesc* __restrict__ Ds, Passes P, int apply_carries) {
+  extern __shared__ __align__(16) uint64_t sm[];
+  const TwoPassDesc& D = Ds[blockIdx.y];
+  const int ld = col_ld((int)D.n2, T);
+  uint32_t status = 0;
+  tile_load(sm, ld, D.x, (int)D.n2, T, D.n1, blockIdx.x * T);
+  __syncthreads();
+  forward_tile<T>(D, P, sm, ld, blockIdx.x, apply_carries != 0, false, status);
+  if (status) atomicOr(D.status, status);
+}
+
+template <int T, int TH>
+__global__ void __launch_bounds__(TH, TH == col_threads<T>() ? col_min_blocks<T>() : 1) col_inverse_r16(
+    const TwoPassDesc* __restrict__ Ds, Passes P, int unsigned_mode) {
+  extern __shared__ __align__(16) uint64_t sm[];
+  const TwoPassDesc& D = Ds[blockIdx.y];
+  const int ld = col_ld((int)D.n2, T);
+  tile_load(sm, ld, D.x, (int)D.n2, T, D.n1, blockIdx.x * T);
+  __syncthreads();
+  inverse_tile<T>(D, P, sm, ld, blockIdx.x, unsigned_mode != 0);
+  tile_store(sm, ld, D.x, (int)D.n2, T, D.n1, blockIdx.x * T);
+}
+
+// ---- carry-fused column kernel: col_inverse of one squaring and col_forward
+// of the next in one launch, the tile staying in shared memory in between.
+//
+// A tile's second half needs the carries of the tile before it (the runs of
+// the same rows).  CTAs take tiles in ticket order (an atomic counter), so the
+// CTA of tile t - 1 has started before the CTA of tile t; every tile publishes
+// its carries with a release flag right after its first half, which waits for
+// nothing, and tile t waits only for tile t - 1's flag.  Tile 0 needs the LAST
+// tile's carries: its CTA waits for the last ticket.  That cannot deadlock:
+// every other CTA waits only for a CTA that is already running, so CTAs keep
+// finishing and the last tile gets a slot; tile 0's second half then runs
+// beside the last tile's.  Flags hold a per-launch epoch, so nothing is
+// cleared between launches.  Every wait is bounded in time and reported.
+//
+// fuse[0]: ticket counter, fuse[1]: epoch, fuse[2 + t]: flag of tile t.
+constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s: far above any launch; then report, never hang
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void publish_flag(uint32_t* flag, uint32_t v) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(flag), "r"(v) : "memory");
+  }
+}
+
+// Thread 0 polls the flag (acquire), the CTA waits at the barrier.  Gives up
+// after kWaitLimitNs, or at once when another CTA already gave up.
+__device__ __forceinline__ void wait_flag(const uint32_t* flag, uint32_t want, uint32_t* status) {
+  if (threadIdx.x == 0) {
+    const uint64_t start = global_ns();
+    uint32_t v = 0, iters = 0;
+    while (true) {
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
+      if (v == want) break;
+      if ((++iters & 63) == 0) {
+        if (*(volatile uint32_t*)status & kStatusFuseTimeout) break;
+        if (global_ns() - start > kWaitLimitNs) {
+          atomicOr(status, kStatusFuseTimeout);
+          break;
+        }
+      }
+      __nanosleep(100);
+    }
+  }
+  __syncthreads();
+}
+
+template <int T, int TH>
+__global__ void __launch_bounds__(TH, TH == col_threads<T>() ? col_min_blocks<T>() : 1) col_fused_r16(
+    const TwoPassDesc* __restrict__ Ds, Passes P) {
+  extern __shared__ __align__(16) uint64_t sm[];
+  __shared__ uint32_t s_ticket, s_epoch;
+  const TwoPassDesc& D = Ds[blockIdx.y];
+  const int L = (int)D.n2, ld = col_ld(L, T);
+  const uint32_t n1 = D.n1, ntiles = D.ntiles;
+  uint32_t* ctl = D.fuse;
+  if (threadIdx.x == 0) {
+    // the epoch is read before the ticket: the last ticket's CTA advances it
+    // only after every CTA of the launch has taken its ticket
+    uint32_t e;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(e) : "l"(ctl + 1) : "memory");
+    s_epoch = e;
+    s_ticket = atomicAdd(ctl, 1u);
+  }
+  __syncthreads();
+  const uint32_t t0 = s_ticket, ready = s_epoch + 1;
+  if (t0 >= ntiles) {  // a counter left over from a launch that did not finish: report, touch nothing
+    if (threadIdx.x == 0) atomicOr(D.status, kStatusFuseTimeout);
+    return;
+  }
+  uint32_t status = 0;
+
+  // first half: inverse column transform of tile t0, carries out
+  tile_load(sm, ld, D.x, L, T, n1, t0 * T);
+  __syncthreads();
+  inverse_tile<T>(D, P, sm, ld, t0, false);
+  publish_flag(ctl + 2 + t0, ready);
+
+  // second half: carries in from the tile before (tile 0: the last tile),
+  // weight, forward column transform
+  wait_flag(ctl + 2 + (t0 > 0 ? t0 - 1 : ntiles - 1), ready, D.status);
+  forward_tile<T>(D, P, sm, ld, t0, true, true, status);
+  if (t0 == ntiles - 1 && threadIdx.x == 0) {
+    // every ticket of this launch is taken and every CTA has read the epoch
+    ctl[0] = 0;
+    __threadfence();
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(ctl + 1), "r"(ready) : "memory");
+  }
+  if (status) atomicOr(D.status, status);
 }
 
 // Raise a kernel's dynamic shared-memory cap once per device (the cap does not
@@ -404,6 +522,37 @@ cudaError_t col_inverse_t(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t 
   col_inverse_r16<T, TH><<<dim3(d.ntiles, count), TH, smem, s>>>(dd, make_passes((int)d.log2n2),
                                                                   unsigned_mode ? 1 : 0);
   return cudaGetLastError();
+}
+
+template <int T, int TH>
+cudaError_t col_fused_t(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count, cudaStream_t s) {
+  const size_t smem = (size_t)T * col_ld((int)d.n2, T) * 8;
+  cudaError_t e = ensure_smem(col_fused_r16<T, TH>, smem);
+  if (e != cudaSuccess) return e;
+  col_fused_r16<T, TH><<<dim3(d.ntiles, count), TH, smem, s>>>(dd, make_passes((int)d.log2n2));
+  return cudaGetLastError();
+}
+
+// Each test of a launch keeps its tile-0 CTA resident while it waits for the
+// test's last tile; at most 128 tests per launch leave most of the GPU's
+// (at least 148) CTA slots to the CTAs those waits depend on, whatever order
+// the hardware dispatches CTAs in.
+constexpr uint32_t kFusedTestsPerLaunch = 128;
+
+cudaError_t launch_col_fused_r16(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
+                                 cudaStream_t s) {
+  for (uint32_t first = 0; first < count; first += kFusedTestsPerLaunch) {
+    const uint32_t c = count - first < kFusedTestsPerLaunch ? count - first : kFusedTestsPerLaunch;
+    cudaError_t e;
+    if (d.tile == 8)
+      e = col_fused_t<8, col_threads<8>()>(d, dd + first, c, s);
+    else if (d.n2 >= 4096)
+      e = col_fused_t<4, col_wide_threads<4>()>(d, dd + first, c, s);
+    else
+      e = col_fused_t<4, col_threads<4>()>(d, dd + first, c, s);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 cudaError_t launch_col_forward_r16(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
