@@ -36,15 +36,16 @@ constexpr int row_threads_for(int L) { return L <= 4096 ? 256 : (L == 8192 ? 512
 // Forward pass of `rows` row transforms.  The first pass (span = L) reads HBM
 // and applies the 4-step twiddle; later passes read shared memory.  One code
 // body serves both, which keeps the kernel small for the instruction cache.
-template <int R>
-__device__ void row_dif_pass(uint64_t* sm, int ld, int rows, int L, int span, const uint64_t* x,
-                             const uint64_t* twf, const uint64_t* twL) {
+template <int R, bool Big>
+__device__ __forceinline__ void row_dif_tasks(uint64_t* sm, int ld, int rows, int L, int span,
+                                              const uint64_t* x, const uint64_t* twf,
+                                              const uint64_t* twL) {
   const bool first = span == L;
-  const int q = span / R, per = L / R;
+  const int q = span / R, per = L / R, qs = q + (q >> 4);
   const int lq = __ffs(q) - 1, lper = __ffs(per) - 1;
   for (int task = threadIdx.x; task < rows * per; task += blockDim.x) {
     const int g = task >> lper, k = task & (per - 1), b = k >> lq, t = k & (q - 1);
-    const int off = b * span + t;
+    const int off = b * span + t, b0 = sw(off);
     uint64_t* base = sm + g * ld;
     uint64_t v[R];
     if (first) {
@@ -53,30 +54,30 @@ __device__ void row_dif_pass(uint64_t* sm, int ld, int rows, int L, int span, co
       for (int d = 0; d < R; ++d) v[d] = gl::mul(x[rb + q * d], twf[rb + q * d]);
     } else {
 #pragma unroll
-      for (int d = 0; d < R; ++d) v[d] = base[sw(off + q * d)];
+      for (int d = 0; d < R; ++d) v[d] = base[task_pos<Big>(b0, q, qs, d)];
     }
     dif<R>(v);
     if (q > 1) mul_task_twiddles<R>(v, twL + t * R);
 #pragma unroll
-    for (int r = 0; r < R; ++r) base[sw(off + q * r)] = v[r];
+    for (int r = 0; r < R; ++r) base[task_pos<Big>(b0, q, qs, r)] = v[r];
   }
 }
 
 // Inverse pass; the last one (span = L) applies the inverse 4-step twiddle and
 // writes HBM.
-template <int R>
-__device__ void row_dit_pass(uint64_t* sm, int ld, int rows, int L, int span, uint64_t* x,
-                             const uint64_t* twi, const uint64_t* itwL) {
+template <int R, bool Big>
+__device__ __forceinline__ void row_dit_tasks(uint64_t* sm, int ld, int rows, int L, int span,
+                                              uint64_t* x, const uint64_t* twi, const uint64_t* itwL) {
   const bool last = span == L;
-  const int q = span / R, per = L / R;
+  const int q = span / R, per = L / R, qs = q + (q >> 4);
   const int lq = __ffs(q) - 1, lper = __ffs(per) - 1;
   for (int task = threadIdx.x; task < rows * per; task += blockDim.x) {
     const int g = task >> lper, k = task & (per - 1), b = k >> lq, t = k & (q - 1);
-    const int off = b * span + t;
+    const int off = b * span + t, b0 = sw(off);
     uint64_t* base = sm + g * ld;
     uint64_t v[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = base[sw(off + q * r)];
+    for (int r = 0; r < R; ++r) v[r] = base[task_pos<Big>(b0, q, qs, r)];
     if (q > 1) mul_task_twiddles<R>(v, itwL + t * R);
     dit_inv<R>(v);
     if (last) {
@@ -85,9 +86,27 @@ __device__ void row_dit_pass(uint64_t* sm, int ld, int rows, int L, int span, ui
       for (int d = 0; d < R; ++d) x[rb + q * d] = gl::mul(v[d], twi[rb + q * d]);
     } else {
 #pragma unroll
-      for (int d = 0; d < R; ++d) base[sw(off + q * d)] = v[d];
+      for (int d = 0; d < R; ++d) base[task_pos<Big>(b0, q, qs, d)] = v[d];
     }
   }
+}
+
+template <int R>
+__device__ void row_dif_pass(uint64_t* sm, int ld, int rows, int L, int span, const uint64_t* x,
+                             const uint64_t* twf, const uint64_t* twL) {
+  if (span / R >= 16)
+    row_dif_tasks<R, true>(sm, ld, rows, L, span, x, twf, twL);
+  else
+    row_dif_tasks<R, false>(sm, ld, rows, L, span, x, twf, twL);
+}
+
+template <int R>
+__device__ void row_dit_pass(uint64_t* sm, int ld, int rows, int L, int span, uint64_t* x,
+                             const uint64_t* twi, const uint64_t* itwL) {
+  if (span / R >= 16)
+    row_dit_tasks<R, true>(sm, ld, rows, L, span, x, twi, itwL);
+  else
+    row_dit_tasks<R, false>(sm, ld, rows, L, span, x, twi, itwL);
 }
 
 template <bool Forward>

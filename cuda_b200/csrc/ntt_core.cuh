@@ -20,37 +20,6 @@
 
 namespace lnt {
 
-#ifndef LNT_SHL_IMAD
-#define LNT_SHL_IMAD 0
-#endif
-
-#if LNT_SHL_IMAD && defined(__CUDACC__)
-// Powers of two from constant memory: the multiplier cannot fold them back
-// into shifts, so the shifted pieces come from the multiplier pipe.
-static __constant__ uint32_t kPow2Words[32] = {
-    1u << 0,  1u << 1,  1u << 2,  1u << 3,  1u << 4,  1u << 5,  1u << 6,  1u << 7,
-    1u << 8,  1u << 9,  1u << 10, 1u << 11, 1u << 12, 1u << 13, 1u << 14, 1u << 15,
-    1u << 16, 1u << 17, 1u << 18, 1u << 19, 1u << 20, 1u << 21, 1u << 22, 1u << 23,
-    1u << 24, 1u << 25, 1u << 26, 1u << 27, 1u << 28, 1u << 29, 1u << 30, 1u << 31};
-
-// x * 2^k (0 < k < 32) as lo (64 bits) + hi * 2^64 (hi < 2^k)
-template <unsigned K>
-__device__ __forceinline__ void mul_pow2_parts(uint64_t x, uint64_t& lo, uint64_t& hi) {
-  const uint32_t m = kPow2Words[K];
-  uint32_t l0, l1, h;
-  asm("{\n\t"
-      "mul.lo.u32 %0, %3, %5;\n\t"
-      "mul.lo.u32 %1, %4, %5;\n\t"
-      "mad.hi.u32 %1, %3, %5, %1;\n\t"
-      "mul.hi.u32 %2, %4, %5;\n\t"
-      "}"
-      : "=r"(l0), "=r"(l1), "=r"(h)
-      : "r"((uint32_t)x), "r"((uint32_t)(x >> 32)), "r"(m));
-  lo = ((uint64_t)l1 << 32) | l0;
-  hi = h;
-}
-#endif
-
 // x * 2^S mod p, 0 <= S < 192, S a compile-time constant.
 template <unsigned S>
 GL_HD uint64_t shl_c(uint64_t x) {
@@ -60,41 +29,16 @@ GL_HD uint64_t shl_c(uint64_t x) {
     return gl::neg(shl_c<S - 96>(x));  // 2^96 = -1
   } else if constexpr (S <= 32) {
     // x 2^S = lo + 2^64 hi with hi < 2^32: lo + hi (2^32 - 1)
-    uint64_t lo, hi;
-#if LNT_SHL_IMAD && defined(__CUDA_ARCH__)
-    if constexpr (S < 32) {
-      mul_pow2_parts<S>(x, lo, hi);
-    } else {
-      lo = x << S;
-      hi = x >> (64 - S);
-    }
-#else
-    lo = x << S;
-    hi = x >> (64 - S);
-#endif
+    const uint64_t lo = x << S, hi = x >> (64 - S);
     const uint64_t m = (hi << 32) - hi;
     uint64_t r = lo + m;
     if (r < m) r += gl::EPS;
     return r >= gl::P ? r - gl::P : r;
   } else if constexpr (S < 64) {
-#if LNT_SHL_IMAD && defined(__CUDA_ARCH__)
-    // x 2^(S-32) = lo + 2^64 hi, then times 2^32: word moves only
-    uint64_t lo, hi;
-    mul_pow2_parts<S - 32>(x, lo, hi);
-    return gl::reduce128(lo << 32, (hi << 32) | (lo >> 32));
-#else
     return gl::reduce128(x << S, x >> (64 - S));
-#endif
   } else {
     // x 2^S = (hi 2^64 + lo) 2^64 with (hi, lo) = x 2^k; 2^128 = -2^32
     constexpr unsigned k = S - 64;
-#if LNT_SHL_IMAD && defined(__CUDA_ARCH__)
-    if constexpr (k > 0) {
-      uint64_t lo, hi;
-      mul_pow2_parts<k>(x, lo, hi);
-      return gl::sub(gl::reduce128(0, lo), hi << 32);
-    }
-#endif
     const uint64_t lo = x << k, hi = k ? (x >> ((64 - k) & 63)) : 0;
     return gl::sub(gl::reduce128(0, lo), hi << 32);
   }

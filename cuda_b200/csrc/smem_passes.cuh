@@ -75,28 +75,43 @@ __device__ __forceinline__ void mul_task_twiddles(uint64_t (&v)[R], const uint64
   }
 }
 
+// Shared-memory position of element d (d < R) of a task whose first element is
+// `off` (off = b * span + t, t < q, span = q * R, all powers of two):
+// sw(off + q d) = sw(off) + q d + (q d >> 4), because the low four bits of
+// off + q d never carry out of a padding group of 16 words.  For q >= 16 that
+// is sw(off) + d (q + q / 16): one stride per pass, no per-element index math.
+template <bool Big>
+__device__ __forceinline__ int task_pos(int b0, int q, int qs, int d) {
+  if constexpr (Big) {
+    return b0 + d * qs;
+  } else {
+    const int k = q * d;
+    return b0 + k + (k >> 4);
+  }
+}
+
 // forward: DIF, then omega_span^(t k) (tw: this task's twiddles; unused when q == 1)
-template <int R>
-__device__ __forceinline__ void task_dif(uint64_t* base, int off, int q, const uint64_t* tw) {
+template <int R, bool Big>
+__device__ __forceinline__ void task_dif(uint64_t* base, int b0, int q, int qs, const uint64_t* tw) {
   uint64_t v[R];
 #pragma unroll
-  for (int d = 0; d < R; ++d) v[d] = base[sw(off + q * d)];
+  for (int d = 0; d < R; ++d) v[d] = base[task_pos<Big>(b0, q, qs, d)];
   dif<R>(v);
   if (q > 1) mul_task_twiddles<R>(v, tw);
 #pragma unroll
-  for (int r = 0; r < R; ++r) base[sw(off + q * r)] = v[r];
+  for (int r = 0; r < R; ++r) base[task_pos<Big>(b0, q, qs, r)] = v[r];
 }
 
 // inverse: omega_span^-(t k), then DIT
-template <int R>
-__device__ __forceinline__ void task_dit(uint64_t* base, int off, int q, const uint64_t* itw) {
+template <int R, bool Big>
+__device__ __forceinline__ void task_dit(uint64_t* base, int b0, int q, int qs, const uint64_t* itw) {
   uint64_t v[R];
 #pragma unroll
-  for (int r = 0; r < R; ++r) v[r] = base[sw(off + q * r)];
+  for (int r = 0; r < R; ++r) v[r] = base[task_pos<Big>(b0, q, qs, r)];
   if (q > 1) mul_task_twiddles<R>(v, itw);
   dit_inv<R>(v);
 #pragma unroll
-  for (int d = 0; d < R; ++d) base[sw(off + q * d)] = v[d];
+  for (int d = 0; d < R; ++d) base[task_pos<Big>(b0, q, qs, d)] = v[d];
 }
 
 // Offset of pass j's twiddles in a pass table (the spans of the passes before it).
@@ -109,26 +124,27 @@ __device__ __forceinline__ int pass_table_offset(const Passes& P, int L, int j) 
   return off;
 }
 
-// last forward pass, pointwise square and first inverse pass (contiguous blocks)
+// last forward pass, pointwise square and first inverse pass (a contiguous
+// block of R words starting at a multiple of R: positions sw(off) + d)
 template <int R>
 __device__ __forceinline__ void task_square(uint64_t* base, int off) {
+  uint64_t* p = base + sw(off);
   uint64_t v[R];
 #pragma unroll
-  for (int d = 0; d < R; ++d) v[d] = base[sw(off + d)];
+  for (int d = 0; d < R; ++d) v[d] = p[d];
   dif<R>(v);
 #pragma unroll
   for (int d = 0; d < R; ++d) v[d] = gl::sqr(v[d]);
   dit_inv<R>(v);
 #pragma unroll
-  for (int d = 0; d < R; ++d) base[sw(off + d)] = v[d];
+  for (int d = 0; d < R; ++d) p[d] = v[d];
 }
 
-// A pass over `ntrans` transforms of length L; transform g lives at sm + g * ld.
-// tw: this pass's part of the pass table.
-template <int R, int Mode>  // Mode 0: DIF, 1: DIT, 2: square
-__device__ void pass(uint64_t* sm, int ld, int ntrans, int L, int span, const uint64_t* tw) {
+template <int R, int Mode, bool Big>
+__device__ __forceinline__ void pass_tasks(uint64_t* sm, int ld, int ntrans, int L, int span,
+                                           const uint64_t* tw) {
   // all sizes are powers of two: index arithmetic by shifts and masks
-  const int q = span / R, per = L / R;
+  const int q = span / R, per = L / R, qs = q + (q >> 4);
   const int lq = __ffs(q) - 1, lper = __ffs(per) - 1;
   const int total = ntrans * per;
   for (int task = threadIdx.x; task < total; task += blockDim.x) {
@@ -136,12 +152,22 @@ __device__ void pass(uint64_t* sm, int ld, int ntrans, int L, int span, const ui
     const int b = k >> lq, t = k & (q - 1);
     uint64_t* base = sm + g * ld;
     if constexpr (Mode == 0)
-      task_dif<R>(base, b * span + t, q, tw + t * R);
+      task_dif<R, Big>(base, sw(b * span + t), q, qs, tw + t * R);
     else if constexpr (Mode == 1)
-      task_dit<R>(base, b * span + t, q, tw + t * R);
+      task_dit<R, Big>(base, sw(b * span + t), q, qs, tw + t * R);
     else
       task_square<R>(base, b * span);
   }
+}
+
+// A pass over `ntrans` transforms of length L; transform g lives at sm + g * ld.
+// tw: this pass's part of the pass table.
+template <int R, int Mode>  // Mode 0: DIF, 1: DIT, 2: square
+__device__ void pass(uint64_t* sm, int ld, int ntrans, int L, int span, const uint64_t* tw) {
+  if (span / R >= 16)
+    pass_tasks<R, Mode, true>(sm, ld, ntrans, L, span, tw);
+  else
+    pass_tasks<R, Mode, false>(sm, ld, ntrans, L, span, tw);
 }
 
 template <int Mode>
