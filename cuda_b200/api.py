@@ -108,6 +108,9 @@ def lib() -> ctypes.CDLL:
         "lnt_batch_poll": ([vp, ctypes.POINTER(BatchResult), i32, ctypes.POINTER(i32)], i32),
         "lnt_batch_status": ([vp, ctypes.POINTER(u32), ctypes.POINTER(u64)], i32),
         "lnt_batch_autotune": ([vp, u32], i32),
+        "lnt_gerbicz_enable": ([vp, u32], i32),
+        "lnt_gerbicz_stats": ([vp, ctypes.POINTER(u64), ctypes.POINTER(u64), ctypes.POINTER(u64)], i32),
+        "lnt_debug_corrupt": ([vp, u32], i32),
         "lnt_batch_use_graphs": ([vp, i32], i32),
     }
     for name, (args, res) in sigs.items():
@@ -258,6 +261,20 @@ class LucasTest:
         o = PlanOptions()
         _check(lib().lnt_get_plan(self._h, ctypes.byref(o)), "lnt_get_plan")
         return o.as_tuple()
+
+    def gerbicz_enable(self, block: int) -> None:
+        """Gerbicz-Li check for PRP tests: verify every block^2 squarings (0: off)."""
+        _check(lib().lnt_gerbicz_enable(self._h, int(block)), "lnt_gerbicz_enable")
+
+    def gerbicz_stats(self) -> dict:
+        v, c, e = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        _check(lib().lnt_gerbicz_stats(self._h, ctypes.byref(v), ctypes.byref(c), ctypes.byref(e)),
+               "lnt_gerbicz_stats")
+        return {"verified_iterations": int(v.value), "checks": int(c.value), "errors": int(e.value)}
+
+    def debug_corrupt(self, word: int = 1) -> None:
+        """Test hook: add 1 to one word of the device state (a simulated hardware error)."""
+        _check(lib().lnt_debug_corrupt(self._h, int(word)), "lnt_debug_corrupt")
 
     def set_stream(self, stream_handle: int | None) -> None:
         _check(lib().lnt_set_stream(self._h, stream_handle), "lnt_set_stream")

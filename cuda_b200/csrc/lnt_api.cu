@@ -18,6 +18,10 @@
 #include "goldilocks.cuh"
 #include "lnt_internal.h"
 
+namespace lnt {
+struct Gerbicz;
+}
+
 struct lnt_test {
   uint32_t q = 0, n = 0;
   int prp = 0;
@@ -61,6 +65,7 @@ struct lnt_test {
   // steady-state squarings of the pass-kernel plan, captured once and replayed
   cudaGraphExec_t graph = nullptr;
   bool graph_failed = false;    // capture unavailable on this stream: plain launches
+  lnt::Gerbicz* gz = nullptr;   // PRP error check (lnt_gerbicz_enable), or none
 };
 
 namespace {
@@ -100,7 +105,10 @@ cudaError_t dalloc(T** p, size_t count) {
   return cudaMalloc((void**)p, count * sizeof(T));
 }
 
+void free_gerbicz(lnt_test* t);
+
 void free_all(lnt_test* t) {
+  free_gerbicz(t);
   void* ptrs[] = {t->x, t->w, t->uw, t->widths, t->status, t->rt, t->irt, t->rdesc, t->tdesc,
                   t->twf, t->twi, t->rt1, t->irt1, t->rt2, t->irt2, t->itw1, t->iitw1,
                   t->itw2, t->iitw2, t->wt, t->uwt, t->widt, t->carry, t->fuse, t->canon,
@@ -474,6 +482,232 @@ int queue_iterations(lnt_test* t, uint64_t iterations, LaunchTimer* timer) {
   return LNT_OK;
 }
 
+// ---- Gerbicz-Li check for PRP tests ---------------------------------------
+//
+// No counterpart in the reference, which checks nothing during a test
+// (lucas_prp.cu:137-195).  With x_i = x_0^(2^i) (the PRP residue after i
+// squarings) and checkpoints c_k = x_{kB} every B squarings, the products
+// D_k = c_0 c_1 ... c_k satisfy D_k = c_0 * D_{k-1}^(2^B).  Every B squarings
+// the engine folds the current residue into D (one residue product); every
+// B^2 squarings it verifies the identity (B squarings of D_{k-1}, one product
+// with c_0, a digit compare).  An error anywhere since the last verification
+// breaks it: the test then returns to the last verified residue and product
+// and redoes the work.  Cost: about 2.5 squarings per B squarings plus B per
+// B^2, under 0.5 % at B = 1000.
+
+}  // namespace
+
+namespace lnt {
+
+// A residue state sharing its test's tables: digits and pending run carries.
+struct StateBuf {
+  int64_t* x = nullptr;
+  int64_t* carry = nullptr;
+  bool canonical_input = true, pending_carries = false, pristine = true, zero_start = false;
+};
+
+struct Gerbicz {
+  uint32_t block = 0;
+  StateBuf c0, d, dprev, v, xok, dok;
+  StateBuf f;                        // scratch: the transformed operand of a product
+  TwoPassDesc* fdesc = nullptr;      // device descriptor of `f`
+  uint64_t done = 0, verified = 0, checks = 0, errors = 0;
+  bool have_prev = false;
+};
+
+}  // namespace lnt
+
+namespace {
+
+size_t carry_words(const lnt_test* t) { return (size_t)t->plan.ntiles * t->plan.n2; }
+
+void free_state(lnt::StateBuf& s) {
+  if (s.x) cudaFree(s.x);
+  if (s.carry) cudaFree(s.carry);
+  s.x = nullptr;
+  s.carry = nullptr;
+}
+
+void free_gerbicz(lnt_test* t) {
+  if (!t->gz) return;
+  lnt::Gerbicz& g = *t->gz;
+  for (lnt::StateBuf* s : {&g.c0, &g.d, &g.dprev, &g.v, &g.xok, &g.dok, &g.f}) free_state(*s);
+  if (g.fdesc) cudaFree(g.fdesc);
+  delete t->gz;
+  t->gz = nullptr;
+}
+
+lnt::StateBuf main_state(const lnt_test* t) {
+  lnt::StateBuf s;
+  s.x = t->x;
+  s.carry = t->carry;
+  s.canonical_input = t->canonical_input;
+  s.pending_carries = t->pending_carries;
+  s.pristine = t->pristine;
+  s.zero_start = t->zero_start;
+  return s;
+}
+
+// Make `s` the test's current state (and the test's state `s`); the device
+// descriptor follows.  Kernels already queued read the descriptor, so the
+// stream is drained first.
+int swap_state(lnt_test* t, lnt::StateBuf& s) {
+  LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
+  std::swap(t->x, s.x);
+  std::swap(t->carry, s.carry);
+  std::swap(t->canonical_input, s.canonical_input);
+  std::swap(t->pending_carries, s.pending_carries);
+  std::swap(t->pristine, s.pristine);
+  std::swap(t->zero_start, s.zero_start);
+  t->canon_valid = false;
+  const lnt::TwoPassDesc hd = twopass_desc(t);
+  LNT_CUDA(cudaMemcpy(t->tdesc, &hd, sizeof(hd), cudaMemcpyHostToDevice), "descriptor");
+  return LNT_OK;
+}
+
+int copy_state(lnt_test* t, lnt::StateBuf& dst, const lnt::StateBuf& src) {
+  LNT_CUDA(cudaMemcpyAsync(dst.x, src.x, (size_t)t->n * 8, cudaMemcpyDeviceToDevice, t->stream), "copy state");
+  LNT_CUDA(cudaMemcpyAsync(dst.carry, src.carry, carry_words(t) * 8, cudaMemcpyDeviceToDevice, t->stream),
+           "copy carries");
+  dst.canonical_input = src.canonical_input;
+  dst.pending_carries = src.pending_carries;
+  dst.pristine = src.pristine;
+  dst.zero_start = src.zero_start;
+  return LNT_OK;
+}
+
+// Copy the test's own state into / out of a buffer.
+int save_main(lnt_test* t, lnt::StateBuf& dst) { return copy_state(t, dst, main_state(t)); }
+int load_main(lnt_test* t, const lnt::StateBuf& src) {
+  lnt::StateBuf m = main_state(t);
+  int st = copy_state(t, m, src);
+  t->canonical_input = src.canonical_input;
+  t->pending_carries = src.pending_carries;
+  t->pristine = src.pristine;
+  t->zero_start = src.zero_start;
+  t->canon_valid = false;
+  return st;
+}
+
+// a <- a * b (a, b: states of this test; b may be the test's own state)
+int mul_state(lnt_test* t, lnt::StateBuf& a, const lnt::StateBuf& b) {
+  lnt::Gerbicz& g = *t->gz;
+  int st;
+  if ((st = copy_state(t, g.f, b)) != LNT_OK) return st;
+  const lnt::TwoPassDesc geo = twopass_desc(t);
+  lnt::TwoPassDesc fd = geo;
+  fd.x = g.f.x;
+  fd.carry = g.f.carry;
+  LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
+  LNT_CUDA(cudaMemcpy(g.fdesc, &fd, sizeof(fd), cudaMemcpyHostToDevice), "descriptor");
+  // the operand's full transform, in place in f
+  LNT_CUDA(lnt::launch_col_forward_r16(geo, g.fdesc, 1, b.pending_carries, t->stream), "col_forward");
+  LNT_CUDA(lnt::launch_row_forward_r16(geo, g.fdesc, t->stream), "row_forward");
+  // a: forward, product with f, inverse, carries
+  const bool both_canonical = a.canonical_input && b.canonical_input;
+  if ((st = swap_state(t, a)) != LNT_OK) return st;
+  const lnt::TwoPassDesc d = twopass_desc(t);
+  cudaError_t e = lnt::launch_col_forward_r16(d, t->tdesc, 1, t->pending_carries, t->stream);
+  if (e == cudaSuccess) e = lnt::launch_row_mul_r16(d, t->tdesc, reinterpret_cast<const uint64_t*>(g.f.x), t->stream);
+  if (e == cudaSuccess) e = lnt::launch_col_inverse_r16(d, t->tdesc, 1, both_canonical, t->stream);
+  t->pending_carries = true;
+  t->canonical_input = false;
+  t->pristine = false;
+  t->zero_start = false;
+  st = swap_state(t, a);
+  if (e != cudaSuccess) return cuda_fail(e, "residue product");
+  return st;
+}
+
+// canonical digits of a state
+int state_digits(lnt_test* t, lnt::StateBuf& s, std::vector<uint64_t>& out) {
+  int st = swap_state(t, s);
+  if (st != LNT_OK) return st;
+  out.resize(t->n);
+  st = canonicalize(t);
+  if (st == LNT_OK) {
+    cudaError_t e = cudaMemcpyAsync(out.data(), t->canon, (size_t)t->n * 8, cudaMemcpyDeviceToHost, t->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(t->stream);
+    if (e != cudaSuccess) st = cuda_fail(e, "read digits");
+  }
+  const int st2 = swap_state(t, s);
+  return st != LNT_OK ? st : st2;
+}
+
+// B squarings of a state
+int square_state(lnt_test* t, lnt::StateBuf& s, uint64_t k) {
+  int st = swap_state(t, s);
+  if (st != LNT_OK) return st;
+  st = queue_iterations(t, k, nullptr);
+  const int st2 = swap_state(t, s);
+  return st != LNT_OK ? st : st2;
+}
+
+// Start (or restart) the chain at the test's current residue.
+int gerbicz_rebase(lnt_test* t) {
+  lnt::Gerbicz& g = *t->gz;
+  int st;
+  for (lnt::StateBuf* s : {&g.c0, &g.d, &g.xok, &g.dok})
+    if ((st = save_main(t, *s)) != LNT_OK) return st;
+  g.done = g.verified = 0;
+  g.have_prev = false;
+  return LNT_OK;
+}
+
+// D_k = c_0 * D_{k-1}^(2^B)?  On success the current residue and product become
+// the verified ones; on failure the test returns to them.
+int gerbicz_verify(lnt_test* t, bool& ok) {
+  lnt::Gerbicz& g = *t->gz;
+  int st;
+  if ((st = copy_state(t, g.v, g.dprev)) != LNT_OK) return st;
+  if ((st = square_state(t, g.v, g.block)) != LNT_OK) return st;
+  if ((st = mul_state(t, g.v, g.c0)) != LNT_OK) return st;
+  std::vector<uint64_t> lhs, rhs;
+  if ((st = state_digits(t, g.d, lhs)) != LNT_OK) return st;
+  if ((st = state_digits(t, g.v, rhs)) != LNT_OK) return st;
+  ok = lhs == rhs;
+  if (ok) {
+    if ((st = save_main(t, g.xok)) != LNT_OK || (st = copy_state(t, g.dok, g.d)) != LNT_OK) return st;
+    g.verified = g.done;
+    ++g.checks;
+  } else {
+    ++g.errors;
+    if ((st = load_main(t, g.xok)) != LNT_OK || (st = copy_state(t, g.d, g.dok)) != LNT_OK) return st;
+    g.done = g.verified;
+    g.have_prev = false;
+  }
+  LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
+  return LNT_OK;
+}
+
+// lnt_iterate with the check: `iterations` squarings that are (up to the last
+// B^2 boundary) verified, redoing blocks that fail.
+int gerbicz_iterate(lnt_test* t, uint64_t iterations) {
+  lnt::Gerbicz& g = *t->gz;
+  const uint64_t B = g.block;
+  uint64_t left = iterations;
+  while (left) {
+    const uint64_t step = std::min<uint64_t>(left, B - g.done % B);
+    int st = queue_iterations(t, step, nullptr);
+    if (st != LNT_OK) return st;
+    g.done += step;
+    left -= step;
+    if (g.done % B != 0) continue;
+    // checkpoint: D_{k-1} kept, D_k = D_{k-1} * x
+    lnt::StateBuf x = main_state(t);
+    if ((st = copy_state(t, g.dprev, g.d)) != LNT_OK) return st;
+    if ((st = mul_state(t, g.d, x)) != LNT_OK) return st;
+    g.have_prev = true;
+    if ((g.done / B) % B == 0) {
+      const uint64_t before = g.done;
+      bool ok = false;
+      if ((st = gerbicz_verify(t, ok)) != LNT_OK) return st;
+      if (!ok) left += before - g.done;  // redo what the failed block covered
+    }
+  }
+  return LNT_OK;
+}
+
 }  // namespace
 
 namespace lnt {
@@ -668,20 +902,73 @@ int lnt_init_test(lnt_test* t) {
   DeviceGuard guard(t->device);
   std::vector<uint64_t> d(t->n, 0);
   d[0] = t->prp ? 3 : 4;
-  return upload_digits(t, d.data());
+  int st = upload_digits(t, d.data());
+  if (st == LNT_OK && t->gz) st = gerbicz_rebase(t);
+  return st;
 }
 
 int lnt_set_digits(lnt_test* t, const uint64_t* digits, size_t n) {
   if (!t || !digits || n != t->n) return fail(LNT_ERR_INVALID_ARGUMENT, "digits/length mismatch");
   DeviceGuard guard(t->device);
-  return upload_digits(t, digits);
+  int st = upload_digits(t, digits);
+  if (st == LNT_OK && t->gz) st = gerbicz_rebase(t);
+  return st;
 }
 
 int lnt_iterate(lnt_test* t, uint64_t iterations) {
   if (!t) return fail(LNT_ERR_INVALID_ARGUMENT, "null test");
   if (iterations == 0) return LNT_OK;
   DeviceGuard guard(t->device);
+  if (t->gz) return gerbicz_iterate(t, iterations);
   return queue_iterations(t, iterations, nullptr);
+}
+
+int lnt_gerbicz_enable(lnt_test* t, uint32_t block) {
+  if (!t) return fail(LNT_ERR_INVALID_ARGUMENT, "null test");
+  DeviceGuard guard(t->device);
+  if (block == 0) {
+    free_gerbicz(t);
+    return LNT_OK;
+  }
+  if (!t->prp) return fail(LNT_ERR_INVALID_ARGUMENT, "the Gerbicz check applies to PRP tests");
+  if (block < 2) return fail(LNT_ERR_INVALID_ARGUMENT, "block must be >= 2");
+  if (t->plan.kind != lnt::PlanKind::TwoPass || !t->plan.fast)
+    return fail(LNT_ERR_UNSUPPORTED_LENGTH, "the Gerbicz check needs a two-pass register-pass plan (n >= 8192)");
+  free_gerbicz(t);
+  t->gz = new lnt::Gerbicz();
+  lnt::Gerbicz& g = *t->gz;
+  g.block = block;
+  cudaError_t e = cudaSuccess;
+  for (lnt::StateBuf* s : {&g.c0, &g.d, &g.dprev, &g.v, &g.xok, &g.dok, &g.f})
+    if (e == cudaSuccess && ((e = dalloc(&s->x, t->n)) == cudaSuccess)) e = dalloc(&s->carry, carry_words(t));
+  if (e == cudaSuccess) e = dalloc(&g.fdesc, 1);
+  if (e != cudaSuccess) {
+    free_gerbicz(t);
+    return cuda_fail(e, "allocate Gerbicz states");
+  }
+  const int st = gerbicz_rebase(t);
+  if (st != LNT_OK) free_gerbicz(t);
+  return st;
+}
+
+int lnt_gerbicz_stats(lnt_test* t, uint64_t* verified_iterations, uint64_t* checks, uint64_t* errors) {
+  if (!t || !t->gz) return fail(LNT_ERR_INVALID_ARGUMENT, "no Gerbicz check on this test");
+  if (verified_iterations) *verified_iterations = t->gz->verified;
+  if (checks) *checks = t->gz->checks;
+  if (errors) *errors = t->gz->errors;
+  return LNT_OK;
+}
+
+int lnt_debug_corrupt(lnt_test* t, uint32_t word) {
+  if (!t || word >= t->n) return fail(LNT_ERR_INVALID_ARGUMENT, "word out of range");
+  DeviceGuard guard(t->device);
+  LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
+  int64_t v = 0;
+  LNT_CUDA(cudaMemcpy(&v, t->x + word, 8, cudaMemcpyDeviceToHost), "read word");
+  v += 1;
+  LNT_CUDA(cudaMemcpy(t->x + word, &v, 8, cudaMemcpyHostToDevice), "write word");
+  t->canon_valid = false;
+  return LNT_OK;
 }
 
 int lnt_profile_iterations(lnt_test* t, uint64_t iterations, lnt_kernel_time* out, int cap,

@@ -131,6 +131,12 @@ cudaError_t launch_row_square_r16(const TwoPassDesc& d, const TwoPassDesc* dd, u
                                   cudaStream_t s);
 cudaError_t launch_col_inverse_r16(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
                                    bool unsigned_mode, cudaStream_t s);
+// product of two residues (one test each, count 1): row_forward_r16 turns a
+// col_forward'ed residue into its full transform F (in place); row_mul_r16 is
+// row_square_r16 with the square replaced by the pointwise product with F
+cudaError_t launch_row_forward_r16(const TwoPassDesc& d, const TwoPassDesc* dd, cudaStream_t s);
+cudaError_t launch_row_mul_r16(const TwoPassDesc& d, const TwoPassDesc* dd, const uint64_t* F,
+                               cudaStream_t s);
 // col_inverse of one squaring and col_forward of the next (steady state: carries
 // pending, signed outputs) in one launch
 cudaError_t launch_col_fused_r16(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,

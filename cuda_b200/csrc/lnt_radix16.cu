@@ -91,10 +91,14 @@ __device__ __forceinline__ void row_dit_tasks(uint64_t* sm, int ld, int rows, in
   }
 }
 
+#ifndef LNT_ROW_STRIDED
+#define LNT_ROW_STRIDED 1
+#endif
+
 template <int R>
 __device__ void row_dif_pass(uint64_t* sm, int ld, int rows, int L, int span, const uint64_t* x,
                              const uint64_t* twf, const uint64_t* twL) {
-  if (span / R >= 16)
+  if (LNT_ROW_STRIDED && span / R >= 16)
     row_dif_tasks<R, true>(sm, ld, rows, L, span, x, twf, twL);
   else
     row_dif_tasks<R, false>(sm, ld, rows, L, span, x, twf, twL);
@@ -103,7 +107,7 @@ __device__ void row_dif_pass(uint64_t* sm, int ld, int rows, int L, int span, co
 template <int R>
 __device__ void row_dit_pass(uint64_t* sm, int ld, int rows, int L, int span, uint64_t* x,
                              const uint64_t* twi, const uint64_t* itwL) {
-  if (span / R >= 16)
+  if (LNT_ROW_STRIDED && span / R >= 16)
     row_dit_tasks<R, true>(sm, ld, rows, L, span, x, twi, itwL);
   else
     row_dit_tasks<R, false>(sm, ld, rows, L, span, x, twi, itwL);
@@ -156,6 +160,57 @@ __global__ void __launch_bounds__(TH, TH == 256 ? LNT_ROW_MIN_BLOCKS : 1024 / TH
   }
 }
 
+// Forward row transforms only (the first half of row_square_r16): the rows
+// after all forward passes, in the order the passes leave them, go back to x.
+// With col_forward before it this is the full transform of a residue, the
+// operand of a product (row_mul_r16).
+template <int TH>
+__global__ void __launch_bounds__(TH) row_forward_r16(const TwoPassDesc* __restrict__ Ds, Passes P, int rows) {
+  extern __shared__ __align__(16) uint64_t sm[];
+  const TwoPassDesc& D = Ds[blockIdx.y];
+  const int L = (int)D.n1, ld = padded(L);
+  const size_t off = (size_t)blockIdx.x * rows * L;
+  uint64_t* x = reinterpret_cast<uint64_t*>(D.x) + off;
+  int span = L;
+  for (int j = 0, seg = 0; j < P.m; ++j) {
+    row_pass_r<true>(P.radix[j], sm, ld, rows, L, span, x, D.twf + off, D.itw1 + seg);
+    seg += span;
+    span /= P.radix[j];
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < rows * L; i += TH) {
+    const int g = i / L, k = i - g * L;
+    x[i] = sm[g * ld + sw(k)];
+  }
+}
+
+// row_square_r16 with the pointwise square replaced by the product with the
+// transformed rows F of another residue (row_forward_r16's output).
+template <int TH>
+__global__ void __launch_bounds__(TH) row_mul_r16(const TwoPassDesc* __restrict__ Ds, Passes P, int rows,
+                                                  const uint64_t* __restrict__ F) {
+  extern __shared__ __align__(16) uint64_t sm[];
+  const TwoPassDesc& D = Ds[blockIdx.y];
+  const int L = (int)D.n1, ld = padded(L);
+  const size_t off = (size_t)blockIdx.x * rows * L;
+  uint64_t* x = reinterpret_cast<uint64_t*>(D.x) + off;
+  int span = L;
+  for (int j = 0, seg = 0; j + 1 < P.m; ++j) {
+    row_pass_r<true>(P.radix[j], sm, ld, rows, L, span, x, D.twf + off, D.itw1 + seg);
+    seg += span;
+    span /= P.radix[j];
+    __syncthreads();
+  }
+  pass_r<3>(P.radix[P.m - 1], sm, ld, rows, L, span, F + off);
+  __syncthreads();
+  for (int j = P.m - 2; j >= 0; --j) {
+    span *= P.radix[j];
+    row_pass_r<false>(P.radix[j], sm, ld, rows, L, span, x, D.twi + off,
+                      D.iitw1 + pass_table_offset(P, L, j));
+    if (j) __syncthreads();
+  }
+}
+
 // --------------------------------------------------------------- columns ----
 
 // column CTAs: 128 threads per tile column (T = 8: 1024 threads, T = 4: 512)
@@ -177,35 +232,50 @@ __host__ __device__ constexpr int col_ld(int L, int T) {
 // 8-byte cp.async, so all of a thread's loads are in flight together.
 __device__ __forceinline__ void tile_load(uint64_t* sm, int ld, const int64_t* x, int L, int T,
                                           uint32_t n1, uint32_t c0) {
-  for (int idx = threadIdx.x; idx < T * L; idx += blockDim.x) {
-    const int r = idx / T, c = idx % T;
-    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(sm + c * ld + sw(r));
-    const int64_t* src = x + (size_t)r * n1 + c0 + c;
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src) : "memory");
+  const int rs = blockDim.x / T;  // rows per round
+  if (blockDim.x % T == 0 && rs % 16 == 0) {
+    // fixed column per thread, rows a constant stride apart: both addresses
+    // advance by a constant (sw(r + rs) = sw(r) + rs + rs / 16)
+    const int c = threadIdx.x % T, r0 = threadIdx.x / T;
+    const int64_t* src = x + (size_t)r0 * n1 + c0 + c;
+    uint32_t dst = (uint32_t)__cvta_generic_to_shared(sm + c * ld + sw(r0));
+    const size_t src_step = (size_t)rs * n1;
+    const uint32_t dst_step = (uint32_t)(rs + rs / 16) * 8;
+    for (int r = r0; r < L; r += rs, src += src_step, dst += dst_step)
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src) : "memory");
+  } else {
+    for (int idx = threadIdx.x; idx < T * L; idx += blockDim.x) {
+      const int r = idx / T, c = idx % T;
+      const uint32_t dst = (uint32_t)__cvta_generic_to_shared(sm + c * ld + sw(r));
+      const int64_t* src = x + (size_t)r * n1 + c0 + c;
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src) : "memory");
+    }
   }
   asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
-// shared memory -> HBM, four words per thread per round so the shared-memory
-// reads overlap
+// shared memory -> HBM: as tile_load, four rounds per loop iteration so the
+// shared-memory reads overlap
 __device__ __forceinline__ void tile_store(const uint64_t* sm, int ld, int64_t* x, int L, int T,
                                            uint32_t n1, uint32_t c0) {
-  const int total = T * L, step = blockDim.x;
-  if (total % (4 * step) != 0) {
-    for (int idx = threadIdx.x; idx < total; idx += step)
-      x[(size_t)(idx / T) * n1 + c0 + idx % T] = (int64_t)sm[(idx % T) * ld + sw(idx / T)];
+  const int rs = blockDim.x / T;
+  if (blockDim.x % T == 0 && rs % 16 == 0 && L % (4 * rs) == 0) {
+    const int c = threadIdx.x % T, r0 = threadIdx.x / T;
+    int64_t* dst = x + (size_t)r0 * n1 + c0 + c;
+    const uint64_t* src = sm + c * ld + sw(r0);
+    const size_t dst_step = (size_t)rs * n1;
+    const int src_step = rs + rs / 16;
+    for (int r = r0; r < L; r += 4 * rs, dst += 4 * dst_step, src += 4 * src_step) {
+      const uint64_t v0 = src[0], v1 = src[src_step], v2 = src[2 * src_step], v3 = src[3 * src_step];
+      dst[0] = (int64_t)v0;
+      dst[dst_step] = (int64_t)v1;
+      dst[2 * dst_step] = (int64_t)v2;
+      dst[3 * dst_step] = (int64_t)v3;
+    }
     return;
   }
-  for (int base = threadIdx.x; base < total; base += 4 * step) {
-    const uint64_t v0 = sm[(base % T) * ld + sw(base / T)];
-    const uint64_t v1 = sm[((base + step) % T) * ld + sw((base + step) / T)];
-    const uint64_t v2 = sm[((base + 2 * step) % T) * ld + sw((base + 2 * step) / T)];
-    const uint64_t v3 = sm[((base + 3 * step) % T) * ld + sw((base + 3 * step) / T)];
-    x[(size_t)(base / T) * n1 + c0 + base % T] = (int64_t)v0;
-    x[(size_t)((base + step) / T) * n1 + c0 + (base + step) % T] = (int64_t)v1;
-    x[(size_t)((base + 2 * step) / T) * n1 + c0 + (base + 2 * step) % T] = (int64_t)v2;
-    x[(size_t)((base + 3 * step) / T) * n1 + c0 + (base + 3 * step) % T] = (int64_t)v3;
-  }
+  for (int idx = threadIdx.x; idx < T * L; idx += blockDim.x)
+    x[(size_t)(idx / T) * n1 + c0 + idx % T] = (int64_t)sm[(idx % T) * ld + sw(idx / T)];
 }
 
 // A row's run of T table entries, read as 16-byte vectors (tile-major tables:
@@ -506,6 +576,43 @@ cudaError_t row_square_t(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t c
   if (e != cudaSuccess) return e;
   row_square_r16<TH><<<dim3(d.n2 / rows, count), TH, smem, s>>>(dd, make_passes((int)d.log2n1), rows);
   return cudaGetLastError();
+}
+
+template <int TH>
+cudaError_t row_forward_t(const TwoPassDesc& d, const TwoPassDesc* dd, cudaStream_t s) {
+  const int L = (int)d.n1, rows = row_rows_per_cta(L, (int)d.n2);
+  const size_t smem = (size_t)rows * padded(L) * 8;
+  cudaError_t e = ensure_smem(row_forward_r16<TH>, smem);
+  if (e != cudaSuccess) return e;
+  row_forward_r16<TH><<<dim3(d.n2 / rows, 1), TH, smem, s>>>(dd, make_passes((int)d.log2n1), rows);
+  return cudaGetLastError();
+}
+
+template <int TH>
+cudaError_t row_mul_t(const TwoPassDesc& d, const TwoPassDesc* dd, const uint64_t* F, cudaStream_t s) {
+  const int L = (int)d.n1, rows = row_rows_per_cta(L, (int)d.n2);
+  const size_t smem = (size_t)rows * padded(L) * 8;
+  cudaError_t e = ensure_smem(row_mul_r16<TH>, smem);
+  if (e != cudaSuccess) return e;
+  row_mul_r16<TH><<<dim3(d.n2 / rows, 1), TH, smem, s>>>(dd, make_passes((int)d.log2n1), rows, F);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_row_forward_r16(const TwoPassDesc& d, const TwoPassDesc* dd, cudaStream_t s) {
+  switch (row_threads_for((int)d.n1)) {
+    case 256: return row_forward_t<256>(d, dd, s);
+    case 512: return row_forward_t<512>(d, dd, s);
+    default: return row_forward_t<1024>(d, dd, s);
+  }
+}
+
+cudaError_t launch_row_mul_r16(const TwoPassDesc& d, const TwoPassDesc* dd, const uint64_t* F,
+                               cudaStream_t s) {
+  switch (row_threads_for((int)d.n1)) {
+    case 256: return row_mul_t<256>(d, dd, F, s);
+    case 512: return row_mul_t<512>(d, dd, F, s);
+    default: return row_mul_t<1024>(d, dd, F, s);
+  }
 }
 
 cudaError_t launch_row_square_r16(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,

@@ -140,6 +140,22 @@ __device__ __forceinline__ void task_square(uint64_t* base, int off) {
   for (int d = 0; d < R; ++d) p[d] = v[d];
 }
 
+// last forward pass, pointwise product with a transformed operand f (the same
+// positions of the same row, in HBM) and first inverse pass
+template <int R>
+__device__ __forceinline__ void task_mul(uint64_t* base, int off, const uint64_t* f) {
+  uint64_t* p = base + sw(off);
+  uint64_t v[R];
+#pragma unroll
+  for (int d = 0; d < R; ++d) v[d] = p[d];
+  dif<R>(v);
+#pragma unroll
+  for (int d = 0; d < R; ++d) v[d] = gl::mul(v[d], f[off + d]);
+  dit_inv<R>(v);
+#pragma unroll
+  for (int d = 0; d < R; ++d) p[d] = v[d];
+}
+
 template <int R, int Mode, bool Big>
 __device__ __forceinline__ void pass_tasks(uint64_t* sm, int ld, int ntrans, int L, int span,
                                            const uint64_t* tw) {
@@ -155,14 +171,17 @@ __device__ __forceinline__ void pass_tasks(uint64_t* sm, int ld, int ntrans, int
       task_dif<R, Big>(base, sw(b * span + t), q, qs, tw + t * R);
     else if constexpr (Mode == 1)
       task_dit<R, Big>(base, sw(b * span + t), q, qs, tw + t * R);
-    else
+    else if constexpr (Mode == 2)
       task_square<R>(base, b * span);
+    else
+      task_mul<R>(base, b * span, tw + (size_t)g * L);
   }
 }
 
 // A pass over `ntrans` transforms of length L; transform g lives at sm + g * ld.
 // tw: this pass's part of the pass table.
-template <int R, int Mode>  // Mode 0: DIF, 1: DIT, 2: square
+// Mode 0: DIF, 1: DIT, 2: square, 3: product with the transformed rows at tw
+template <int R, int Mode>
 __device__ void pass(uint64_t* sm, int ld, int ntrans, int L, int span, const uint64_t* tw) {
   if (span / R >= 16)
     pass_tasks<R, Mode, true>(sm, ld, ntrans, L, span, tw);

@@ -83,7 +83,7 @@ typedef enum lnt_plan_kind {
   LNT_PLAN_AUTO = 0,     /* the policy's choice */
   LNT_PLAN_RESIDENT = 1, /* n <= 4096: one CTA per residue, state in shared memory (FFT_1SMEM) */
   LNT_PLAN_RADIX16 = 2,  /* 4-step columns x rows, register passes of radix <= 16 (FFT_2SMEM family) */
-  LNT_PLAN_RADIX2 = 3    /* 4-step columns x rows, radix-2 stages (the only one for 2^25, 2^26) */
+  LNT_PLAN_RADIX2 = 3    /* 4-step columns x rows, radix-2 stages (the first kernels; an explicit plan) */
 } lnt_plan_kind;
 
 typedef struct lnt_plan_options {
@@ -149,6 +149,28 @@ int lnt_res64(lnt_test* t, uint64_t* res64);
 /* Verdict of LucasPRP::Run (lucas_prp.cu:167-184): *is_prime = 1 when the
  * residue is 0 (LL) or 9 (PRP). Meaningful after the full test. */
 int lnt_is_prime(lnt_test* t, int* is_prime);
+
+/* ---- Gerbicz-Li error check (PRP) --------------------------------------------
+ * No counterpart in the reference, which checks nothing during a test
+ * (lucas_prp.cu:137-195).  For PRP tests on two-pass plans (n >= 8192):
+ * every `block` squarings lnt_iterate folds the residue into a running
+ * product D of checkpoint residues, and every block^2 squarings it verifies
+ * D_k = x_0 * D_{k-1}^(2^block); on a mismatch it returns to the last verified
+ * residue and redoes the work, so the residues it returns are the error-free
+ * ones up to the last verification.  Costs about 2.5 squarings per block plus
+ * `block` per block^2 (under 0.5 % at block = 1000) and 7 residue-sized
+ * buffers.  lnt_set_digits / lnt_init_test restart the chain.
+ * block = 0 turns the check off.  LNT_ERR_INVALID_ARGUMENT for LL tests,
+ * LNT_ERR_UNSUPPORTED_LENGTH for the SMEM-resident and radix-2 plans. */
+int lnt_gerbicz_enable(lnt_test* t, uint32_t block);
+
+/* Squarings verified so far (since enable / the last set_digits), checks
+ * passed and errors detected (each followed by a rollback). */
+int lnt_gerbicz_stats(lnt_test* t, uint64_t* verified_iterations, uint64_t* checks, uint64_t* errors);
+
+/* Diagnostic without a reference counterpart, for tests of the check: adds 1
+ * to word `word` of the device state, as a hardware error would corrupt it. */
+int lnt_debug_corrupt(lnt_test* t, uint32_t word);
 
 /* Length, widths (n bytes, pre_calculation.cu:35) and plan name of a test. */
 int lnt_get_length(lnt_test* t, uint32_t* n);

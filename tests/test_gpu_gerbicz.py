@@ -1,0 +1,70 @@
+"""GPU: the Gerbicz-Li check of PRP tests (lnt_gerbicz_enable).
+
+The check multiplies residues (a product kernel path beside the squaring), so
+it is exercised end to end: a checked PRP test of a Mersenne prime still ends
+with residue 9; a checked test gives the same residue as an unchecked one; and
+a residue word corrupted between calls (what a hardware error would do) is
+detected at the next verification and the test recovers to the error-free
+residue.
+"""
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def plain_res64(lnt, q, iterations):
+    with lnt.LucasTest(q, prp=True) as t:
+        t.iterate(iterations)
+        return t.res64()
+
+
+def test_checked_prp_of_a_mersenne_prime(lnt):
+    q = 132049  # M_132049 is prime; n = 8192, a two-pass plan
+    with lnt.LucasTest(q, prp=True) as t:
+        t.gerbicz_enable(64)
+        t.iterate(q)
+        assert t.is_prime() and t.res64() == 9
+        st = t.gerbicz_stats()
+        assert st["errors"] == 0 and st["checks"] == q // (64 * 64)
+        assert st["verified_iterations"] == st["checks"] * 64 * 64
+
+
+@pytest.mark.parametrize("q,block,iterations", [(160001, 32, 20000), (1000003, 40, 9000)])
+def test_checked_equals_unchecked(lnt, q, block, iterations):
+    with lnt.LucasTest(q, prp=True) as t:
+        t.gerbicz_enable(block)
+        for k in (777, iterations - 777):  # calls not aligned to the blocks
+            t.iterate(k)
+        assert t.res64() == plain_res64(lnt, q, iterations)
+        st = t.gerbicz_stats()
+        assert st["errors"] == 0 and st["checks"] == iterations // (block * block)
+
+
+def test_corrupted_word_is_caught_and_undone(lnt):
+    q, block, iterations = 160001, 32, 12000
+    with lnt.LucasTest(q, prp=True) as t:
+        t.gerbicz_enable(block)
+        t.iterate(5000)
+        t.debug_corrupt(17)
+        t.iterate(iterations - 5000)
+        st = t.gerbicz_stats()
+        assert st["errors"] >= 1
+        assert t.res64() == plain_res64(lnt, q, iterations)
+
+
+def test_checked_c2_length(lnt):
+    q, block, iterations = 139000003, 50, 5000  # n = 2^23, two verifications
+    with lnt.LucasTest(q, prp=True) as t:
+        t.gerbicz_enable(block)
+        t.iterate(iterations)
+        assert t.gerbicz_stats()["checks"] == 2
+        assert t.res64() == plain_res64(lnt, q, iterations)
+
+
+def test_check_needs_prp_and_a_two_pass_plan(lnt):
+    with lnt.LucasTest(160001, prp=False) as t:
+        with pytest.raises(lnt.LucasNTTError):
+            t.gerbicz_enable(64)
+    with lnt.LucasTest(9941, prp=True) as t:  # n = 512: SMEM-resident plan
+        with pytest.raises(lnt.LucasNTTError):
+            t.gerbicz_enable(64)
