@@ -79,6 +79,7 @@ void LucasPRP::Run() {
   } else {
     InitializeTest();
   }
+  EnableGerbicz();
   const Clock::time_point t0 = Clock::now();
   MainLoop();
   Check(lnt_synchronize(t_), "lnt_synchronize");
@@ -104,6 +105,18 @@ void LucasPRP::Run() {
   if (o_.dump_residue || interrupted_ || current_iteration_ + 2 <= o_.exponent) DumpResidue();
   if (o_.dump_environment) DumpEnvironment();
   if (o_.dump_stats) DumpStats(total_ms_);
+}
+
+// The Gerbicz-Li check (GerbiczBlock, an extension) on the residue the loop
+// starts from: a fresh test or the residue a resume loaded.
+void LucasPRP::EnableGerbicz() {
+  if (!o_.prp || o_.gerbicz_block == 0) return;
+  const int st = lnt_gerbicz_enable(t_, o_.gerbicz_block);
+  gerbicz_ = st == LNT_OK;
+  if (gerbicz_)
+    LOG_VERBOSE("Gerbicz check every %u squarings", o_.gerbicz_block * o_.gerbicz_block);
+  else
+    LOG_NORMAL("Gerbicz check not available for this test: %s", lnt_last_error());
 }
 
 void LucasPRP::MainLoop() {
@@ -224,6 +237,8 @@ void LucasPRP::DumpStats(double total_ms) {
   r.total_seconds = total_ms / 1000.0;
   r.has_res64 = true;
   r.res64 = res64_of(host_x_, widths_);
+  if (gerbicz_ && lnt_gerbicz_stats(t_, nullptr, &r.gerbicz_checks, &r.gerbicz_errors) == LNT_OK)
+    r.has_gerbicz = true;
   if (!WriteStatsFile(o_.stat_filename, r))
     LOG_NORMAL("Cannot write the statistics to %s", o_.stat_filename.c_str());
 }

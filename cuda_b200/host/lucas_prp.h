@@ -44,6 +44,7 @@ class LucasPRP : public Process {
   void DumpStats(double total_ms);
   void DumpEnvironment();
   void Check(int status, const char* what);
+  void EnableGerbicz();
 
   MainOptions& o_;
   lnt_plan_options plan_;
@@ -57,6 +58,7 @@ class LucasPRP : public Process {
   bool is_prime_ = false, is_composite_ = false;
   double total_ms_ = 0;
   double ms_per_iteration_estimate_ = 0;
+  bool gerbicz_ = false;
 };
 
 }  // namespace lucasntt

@@ -47,6 +47,10 @@ MainOptions ResolveOptions(int argc, char** argv, const std::string& ini_path) {
   o.dump_environment = ini ? ini->GetLongValue("dumpEnvironment", 0) == 1 : false;
   o.safety_dump_seconds = ini ? (double)ini->GetLongValue("SafetyDumpSeconds", 3600) : 3600.0;
   if (o.safety_dump_seconds <= 0) o.safety_dump_seconds = 3600.0;
+  {
+    const long b = ini ? ini->GetLongValue("GerbiczBlock", 0) : 0;
+    o.gerbicz_block = b > 0 && b < (1L << 20) ? (uint32_t)b : 0;
+  }
 
   // an interrupted run's stats file replaces LucasNTT.ini (main_process.cu:98-106)
   IniFile last;

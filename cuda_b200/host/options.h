@@ -34,6 +34,9 @@ struct MainOptions {
   // Extension: seconds between safety dumps of residue + stats (the
   // reference's fixed hour, lucas_prp.cu:201-215).  Key SafetyDumpSeconds.
   double safety_dump_seconds = 3600.0;
+  // Extension: GerbiczBlock = B turns on the Gerbicz-Li check of PRP tests
+  // (lnt_gerbicz_enable; a verification every B^2 squarings).  0 = off.
+  uint32_t gerbicz_block = 0;
 };
 
 // Resolve the options.  `ini_path` is LucasNTT.ini in the working directory

@@ -107,6 +107,10 @@ bool WriteStatsFile(const std::string& path, const StatsRecord& r) {
     std::fprintf(fp, "Warning! total time is not relevant since the full process has been interrupted by CTRL-C\n");
   std::fprintf(fp, "Total time (sec) = %g\n", r.total_seconds);
   if (r.has_res64) std::fprintf(fp, "Res64 = %016" PRIX64 "\n", r.res64);
+  if (r.has_gerbicz) {
+    std::fprintf(fp, "Gerbicz checks = %" PRIu64 "\n", r.gerbicz_checks);
+    std::fprintf(fp, "Gerbicz errors = %" PRIu64 "\n", r.gerbicz_errors);
+  }
   return std::fclose(fp) == 0;
 }
 

@@ -38,6 +38,8 @@ struct StatsRecord {
   double total_seconds = 0;
   bool has_res64 = false;
   uint64_t res64 = 0;
+  bool has_gerbicz = false;
+  uint64_t gerbicz_checks = 0, gerbicz_errors = 0;
 };
 
 // DumpStats (lucas_prp.cu:293-324): same keys, same order, same %g formats;

@@ -74,6 +74,15 @@ def test_full_prp_probable_prime_and_environment(tmp_path):
     assert "CUDA Version = " in env and "Device 0 = " in env and "Multiprocessors = " in env
 
 
+def test_gerbicz_check_from_the_ini(tmp_path):
+    """GerbiczBlock (an extension key): a checked PRP of M_132049, checks in the stats file."""
+    r = run_cli(tmp_path, [132049, 0, "g"], ini="PRP = 1\nPerformanceLoops = 50\nGerbiczBlock = 64\n")
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "M(132049) is probably prime!" in r.stdout
+    s = stats(tmp_path / "g.txt")
+    assert s["Gerbicz checks"] == str(132049 // 4096) and s["Gerbicz errors"] == "0"
+
+
 def test_composite_verdict(tmp_path):
     r = run_cli(tmp_path, [9973, 0, "c"], ini="PerformanceLoops = 50\n")
     assert r.returncode == 0 and "M(9973) is composite!" in r.stdout
