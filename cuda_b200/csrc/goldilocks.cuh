@@ -101,6 +101,76 @@ GL_HD uint64_t add(uint64_t a, uint64_t b) {
 
 GL_HD uint64_t neg(uint64_t a) { return a ? P - a : 0; }
 
+// LNT_GL_MUL selects the device reductions: 1 (default) reduce_words below,
+// with the product r2 (2^32 - 1) on the multiplier pipe, which the
+// integer-bound kernels leave mostly idle; 0 the add/sub chains of mul
+// (r2 (2^32 - 1) from two subtractions).  At n = 2^23: 462.5 us per squaring
+// with 1, 519.4 with 0; 1 with the 128-bit product from four 32 x 32 -> 64
+// multiply-adds instead of the mad chain of mul: 471.6.
+#ifndef LNT_GL_MUL
+#define LNT_GL_MUL 1
+#endif
+
+#if defined(__CUDA_ARCH__)
+// (t1:t0) in [0, 2^64) to [0, p): a value >= p has the high word 2^32 - 1 and
+// a non-zero low word, and minus p it is the low word minus one.
+__device__ __forceinline__ uint64_t canon_words(uint32_t t0, uint32_t t1) {
+  if (t1 == 0xFFFFFFFFu && t0 != 0u) {
+    t0 -= 1u;
+    t1 = 0u;
+  }
+  return ((uint64_t)t1 << 32) | t0;
+}
+
+// r0 + r1 2^32 + r2 2^64 + r3 2^96 mod p for any 32-bit words, canonical:
+// (r1:r0) + r2 (2^32 - 1) - r3 (2^64 = 2^32 - 1, 2^96 = -1).  The first sum
+// runs on the multiplier (mad with carry); with c its carry and b the borrow
+// of the subtraction the value is the 64-bit word plus (c - b)(2^32 - 1).
+// That correction cannot overflow (c = 1 leaves at most 2^64 - 2^33) nor
+// underflow (b = 1 leaves at least p), and its result is below p, so only
+// c = b can leave a word >= p for canon_words.
+__device__ __forceinline__ uint64_t reduce_words(uint32_t r0, uint32_t r1, uint32_t r2,
+                                                 uint32_t r3) {
+  uint32_t t0, t1;
+  asm("{\n\t"
+      ".reg .u32 cm, b, lo, hi;\n\t"
+      "mad.lo.cc.u32  %0, %4, 0xFFFFFFFF, %2;\n\t"
+      "madc.hi.cc.u32 %1, %4, 0xFFFFFFFF, %3;\n\t"
+      "addc.u32       cm, 0xFFFFFFFF, 0;\n\t"  // c - 1
+      "sub.cc.u32     %0, %0, %5;\n\t"
+      "subc.cc.u32    %1, %1, 0;\n\t"
+      "subc.u32       b, 0, 0;\n\t"            // -b
+      "sub.u32        lo, 0xFFFFFFFF, cm;\n\t"
+      "sub.u32        lo, lo, b;\n\t"          // low word of (c - b)(2^32 - 1): b - c
+      "and.b32        hi, b, cm;\n\t"          // high word: all ones iff c - b = -1
+      "add.cc.u32     %0, %0, lo;\n\t"
+      "addc.u32       %1, %1, hi;\n\t"
+      "}"
+      : "=r"(t0), "=r"(t1)
+      : "r"(r0), "r"(r1), "r"(r2), "r"(r3));
+  return canon_words(t0, t1);
+}
+
+// r0 + r1 2^32 + r2 2^64 mod p: (r1:r0) + r2 (2^32 - 1) on the multiplier,
+// its carry c folded back as c 2^32 - c (c = 1 leaves at most (2^32 - 1)^2 - 1,
+// so neither step wraps and the result is below p).
+__device__ __forceinline__ uint64_t reduce_words3(uint32_t r0, uint32_t r1, uint32_t r2) {
+  uint32_t t0, t1;
+  asm("{\n\t"
+      ".reg .u32 c;\n\t"
+      "mad.lo.cc.u32  %0, %4, 0xFFFFFFFF, %2;\n\t"
+      "madc.hi.cc.u32 %1, %4, 0xFFFFFFFF, %3;\n\t"
+      "addc.u32       c, 0, 0;\n\t"
+      "add.u32        %1, %1, c;\n\t"
+      "sub.cc.u32     %0, %0, c;\n\t"
+      "subc.u32       %1, %1, 0;\n\t"
+      "}"
+      : "=r"(t0), "=r"(t1)
+      : "r"(r0), "r"(r1), "r"(r2));
+  return canon_words(t0, t1);
+}
+#endif
+
 // lo + 2^64 * hi, with hi = h1 * 2^32 + h0, is lo + h0 * (2^32 - 1) - h1.
 GL_HD uint64_t reduce128(uint64_t lo, uint64_t hi) {
   uint64_t h1 = hi >> 32, h0 = hi & 0xFFFFFFFFull;
@@ -115,7 +185,7 @@ GL_HD uint64_t reduce128(uint64_t lo, uint64_t hi) {
 GL_HD uint64_t mul(uint64_t a, uint64_t b) {
 #if defined(__CUDA_ARCH__)
   // 128-bit product from 32-bit limbs (multiplier pipe), then the reduction
-  // lo + r2 (2^32 - 1) - r3 with carry chains.
+  // lo + r2 (2^32 - 1) - r3.
   uint32_t r0, r1, r2, r3;
   asm("{\n\t"
       "mul.lo.u32     %0, %4, %6;\n\t"
@@ -130,6 +200,9 @@ GL_HD uint64_t mul(uint64_t a, uint64_t b) {
       "}"
       : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
       : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)), "r"((uint32_t)b), "r"((uint32_t)(b >> 32)));
+#if LNT_GL_MUL == 1
+  return reduce_words(r0, r1, r2, r3);
+#else
 #if LNT_GL_SHORT
   // t = (r1:r0) - r3 (borrow: minus the mask 2^32 - 1, as sub_chain), then
   // t + r2 (2^32 - 1) with its carry read by addc and folded back as 2^32 - 1.
@@ -171,6 +244,7 @@ GL_HD uint64_t mul(uint64_t a, uint64_t b) {
 #endif
   const uint64_t r = ((uint64_t)t1 << 32) | t0;
   return r >= P ? r - P : r;
+#endif
 #else
   return reduce128(a * b, mulhi(a, b));
 #endif
@@ -216,7 +290,18 @@ GL_HD uint64_t mul_pow2(uint64_t x, unsigned s) {
 GL_HD uint64_t mul_digit(int64_t d, uint64_t w) {
   const bool negative = d < 0;
   const uint32_t a = (uint32_t)(negative ? -d : d);
-#if defined(__CUDA_ARCH__)
+#if defined(__CUDA_ARCH__) && LNT_GL_MUL >= 1
+  uint32_t r0, r1, r2;
+  asm("{\n\t"
+      "mul.lo.u32     %0, %3, %4;\n\t"
+      "mul.hi.u32     %1, %3, %4;\n\t"
+      "mad.lo.cc.u32  %1, %3, %5, %1;\n\t"
+      "madc.hi.u32    %2, %3, %5, 0;\n\t"
+      "}"
+      : "=r"(r0), "=r"(r1), "=r"(r2)
+      : "r"(a), "r"((uint32_t)w), "r"((uint32_t)(w >> 32)));
+  const uint64_t r = reduce_words3(r0, r1, r2);
+#elif defined(__CUDA_ARCH__)
   uint32_t t0, t1;
   asm("{\n\t"
       ".reg .u32 r2, u0, u1, c, m;\n\t"

@@ -27,6 +27,25 @@ GL_HD uint64_t shl_c(uint64_t x) {
     return x;
   } else if constexpr (S >= 96) {
     return gl::neg(shl_c<S - 96>(x));  // 2^96 = -1
+#if defined(__CUDA_ARCH__) && LNT_GL_MUL >= 1
+    // device: the shifted words, reduced by gl::reduce_words(3)
+  } else if constexpr (S < 32) {
+    const uint64_t lo = x << S;  // + 2^64 (x >> (64 - S)), below 2^32
+    return gl::reduce_words3((uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)(x >> (64 - S)));
+  } else if constexpr (S == 32) {
+    return gl::reduce_words3(0u, (uint32_t)x, (uint32_t)(x >> 32));
+  } else if constexpr (S < 64) {
+    const uint64_t hi = x >> (64 - S);  // x 2^S = (x0 << (S - 32)) 2^32 + hi 2^64
+    return gl::reduce_words(0u, (uint32_t)x << (S - 32), (uint32_t)hi, (uint32_t)(hi >> 32));
+  } else {
+    // x 2^S = y 2^64 + z 2^128 with y = x << k (64 bits), z = x >> (64 - k) < 2^32
+    // (k = S - 64); 2^128 = -2^32 and p - z 2^32 = (2^32 - 1 - z) 2^32 + 1
+    constexpr unsigned k = S - 64;
+    const uint64_t y = x << k;
+    const uint32_t z = k ? (uint32_t)(x >> ((64 - k) & 63)) : 0u;
+    return gl::reduce_words(1u, ~z, (uint32_t)y, (uint32_t)(y >> 32));
+  }
+#else
   } else if constexpr (S <= 32) {
     // x 2^S = lo + 2^64 hi with hi < 2^32: lo + hi (2^32 - 1)
     const uint64_t lo = x << S, hi = x >> (64 - S);
@@ -42,6 +61,7 @@ GL_HD uint64_t shl_c(uint64_t x) {
     const uint64_t lo = x << k, hi = k ? (x >> ((64 - k) & 63)) : 0;
     return gl::sub(gl::reduce128(0, lo), hi << 32);
   }
+#endif
 }
 
 // a*w, b -> (a + b, (a - b) * 2^S): the DIF butterfly with a power-of-two twiddle.
