@@ -59,7 +59,9 @@ __host__ __device__ inline Passes make_passes(int log2L) {
 // ---- one task: R elements of one block, forward or inverse ----------------
 
 // The R twiddles of one task, a 16-byte aligned run of the pass table: read as
-// R/2 vector loads from one base address.
+// R/2 vector loads from one base address.  Element 0's twiddle is
+// omega^(t brev(0)) = 1 in every task: it is loaded (the vector load) but not
+// multiplied.
 #ifndef LNT_TW_UNROLL
 #define LNT_TW_UNROLL 8  // twiddle vectors loaded per unrolled step (register pressure)
 #endif
@@ -70,7 +72,7 @@ __device__ __forceinline__ void mul_task_twiddles(uint64_t (&v)[R], const uint64
 #pragma unroll kTwUnroll
   for (int k = 0; k < R / 2; ++k) {
     const ulonglong2 u = __ldg(w2 + k);
-    v[2 * k] = gl::mul(v[2 * k], u.x);
+    if (k > 0) v[2 * k] = gl::mul(v[2 * k], u.x);
     v[2 * k + 1] = gl::mul(v[2 * k + 1], u.y);
   }
 }
