@@ -8,6 +8,7 @@ from .api import (  # noqa: F401
     LucasNTTError,
     LucasTest,
     PlanOptions,
+    arith_selftest,
     autotune,
     check_provided_length,
     length_candidates,

@@ -112,6 +112,7 @@ def lib() -> ctypes.CDLL:
         "lnt_gerbicz_stats": ([vp, ctypes.POINTER(u64), ctypes.POINTER(u64), ctypes.POINTER(u64)], i32),
         "lnt_debug_corrupt": ([vp, u32], i32),
         "lnt_batch_use_graphs": ([vp, i32], i32),
+        "lnt_arith_selftest": ([i32, ctypes.POINTER(u64), ctypes.POINTER(u64)], i32),
     }
     for name, (args, res) in sigs.items():
         f = getattr(L, name)
@@ -166,6 +167,15 @@ def plan_describe(plan: tuple[int, int, int], exponent: int, n: int = 0) -> str:
     o = PlanOptions(*plan)
     _check(lib().lnt_plan_describe(ctypes.byref(o), exponent, n, buf, 128), "lnt_plan_describe")
     return buf.value.decode()
+
+
+def arith_selftest(device: int = 0) -> int:
+    """lnt_arith_selftest: the device modular arithmetic against the host build
+    on edge and seeded random operands; returns the number of results checked
+    and raises LucasNTTError (LNT_ERR_NUMERIC) on any mismatch."""
+    checked, bad = ctypes.c_uint64(), ctypes.c_uint64()
+    _check(lib().lnt_arith_selftest(device, ctypes.byref(checked), ctypes.byref(bad)), "lnt_arith_selftest")
+    return int(checked.value)
 
 
 def autotune(exponent: int, n: int = 0, prp: bool = False, device: int = 0, loops: int = 100):

@@ -1111,8 +1111,10 @@ int lnt_time_plans(uint32_t exponent, uint32_t n, int prp, int device, uint32_t 
     if (st == LNT_OK) {
       DeviceGuard guard(t->device);
       cudaEvent_t e0 = nullptr, e1 = nullptr;
-      const uint64_t warm = loops / 10 + 2;
-      if ((st = lnt_iterate(t, warm)) == LNT_OK && (st = lnt_synchronize(t)) == LNT_OK) {
+      // the warm-up is the timed call itself, untimed: it captures the CUDA
+      // graphs and loads the kernels that call uses (the first candidate also
+      // pays the per-device set-up there), so the timed call replays only
+      if ((st = lnt_iterate(t, loops)) == LNT_OK && (st = lnt_synchronize(t)) == LNT_OK) {
         if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess ||
             cudaEventRecord(e0, t->stream) != cudaSuccess)
           st = fail(LNT_ERR_CUDA, "autotune events");

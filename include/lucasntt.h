@@ -112,14 +112,16 @@ int lnt_plan_describe(const lnt_plan_options* plan, uint32_t exponent, uint32_t 
                       size_t outlen);
 
 /* Process::GetBestPerformers (process.cu:45-127): times `loops` squarings of
- * every candidate plan (after a short warm-up) on `device`.  tried[i] / ms[i]
+ * every candidate plan on `device` (as lnt_time_plans).  tried[i] / ms[i]
  * (ms = -1: the candidate failed) for i < min(count, cap); *best indexes the
  * fastest.  Allocates and frees one test at a time. */
 int lnt_autotune(uint32_t exponent, uint32_t n, int prp, int device, uint32_t loops,
                  lnt_plan_options* tried, float* ms, int cap, int* count, int* best);
 
 /* Process::EvaluatePerformance (process.cu:129-149) for a given list of plans:
- * ms[i] = time of `loops` squarings with plans[i], or -1 if it failed. */
+ * ms[i] = time of `loops` squarings with plans[i], or -1 if it failed.  Each
+ * plan runs `loops` squarings untimed first (graph capture, kernel loading),
+ * then the same call timed. */
 int lnt_time_plans(uint32_t exponent, uint32_t n, int prp, int device, uint32_t loops,
                    const lnt_plan_options* plans, int count, float* ms);
 
@@ -180,6 +182,12 @@ int lnt_plan_name(lnt_test* t, char* out, size_t outlen);
 /* LucasPRP::DumpEnvironment (lucas_prp.cu:265-291): the text of the
  * reference's .env file (CUDA version, devices and their properties). */
 int lnt_environment(char* out, size_t outlen);
+
+/* Self-test without a reference counterpart: the device modular arithmetic
+ * (multiply, add, subtract, power-of-two shifts, digit products) on edge and
+ * seeded random operands, each result compared with the host implementation.
+ * LNT_ERR_NUMERIC (first mismatch in lnt_last_error) if any differs. */
+int lnt_arith_selftest(int device, uint64_t* checked, uint64_t* mismatches);
 
 /* Run the test's work on a caller-owned cudaStream_t (NULL = the test's own
  * stream), the analogue of common::stream (common/common.cu:118). */

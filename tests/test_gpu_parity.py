@@ -168,3 +168,11 @@ def test_reference_build_residues(lnt):
             T.iterate(c["iterations"] - done)
             done = c["iterations"]
             assert f"{T.res64():016x}" == c["res64"], c
+
+
+def test_device_arithmetic_against_host(lnt):
+    """The device reductions (multiplier-pipe sums, canonical step, shift
+    twiddles, digit products) equal the host build on edge operands that reach
+    their rare branches and on seeded random operands."""
+    checked = lnt.arith_selftest(0)
+    assert checked == (25 * 25 + 3 * 8192) * 16
