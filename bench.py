@@ -50,8 +50,9 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--iterations-per-step", type=int, default=ITERATIONS_PER_STEP)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["c1", "c2", "c3", "c4", "c5"], default="c2",
-                    help="c2: one 8M-point LL test (default); c3/c4: batched tests/hour; c5: serving")
+    ap.add_argument("--workload", choices=["c1", "c2", "c3", "c4", "c5", "lengths"], default="c2",
+                    help="c2: one 8M-point LL test (default); c3/c4: batched tests/hour; c5: serving; "
+                         "lengths: one LL test at each of 2^24, 2^25, 2^26")
     ap.add_argument("--seconds", type=float, default=30.0, help="timed window of c3/c4/c5")
     ap.add_argument("--rates", default="0.5,1,2", help="c5: arrival rates as multiples of plain capacity")
     ap.add_argument("--c5-range", default="10000,200000",
@@ -209,6 +210,46 @@ def reference_us_per_iteration() -> dict:
         return {}
     d = json.loads(p.read_text())["by_n"]
     return {int(n): min(r["per_iteration_us"] for r in runs) for n, runs in d.items()}
+
+
+LENGTH_EXPONENTS = [300000007, 600000001, 1100000009]  # policy lengths 2^24, 2^25, 2^26
+
+
+def run_lengths(args):
+    """One LL test alone at each larger policy length: µs per squaring from
+    CUDA events on the test's stream around `--iterations-per-step` squarings
+    (after `--warmup` untimed calls of the same size), the kernel split of one
+    more call, and the reference build's time at that length."""
+    import torch
+
+    import cuda_b200
+
+    ref = reference_us_per_iteration()
+    ips = min(args.iterations_per_step, 200)
+    for q in LENGTH_EXPONENTS:
+        stream = torch.cuda.Stream()
+        with cuda_b200.LucasTest(q) as t:
+            t.set_stream(stream.cuda_stream)
+            for _ in range(max(args.warmup, 1)):
+                t.iterate(ips)
+            stream.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            t.iterate(ips)
+            e1.record(stream)
+            stream.synchronize()
+            us = e0.elapsed_time(e1) * 1e3 / ips
+            prof = t.profile_iterations(ips)
+            n = 1 << cuda_b200.secured_log2_length(q)
+            line = {"metric": f"us/iteration, LL q={q} at n=2^{n.bit_length() - 1}", "value": us,
+                    "unit": "us/iteration", "higher_is_better": False, "n_gpus": 1, "dtype": "u64",
+                    "data": "LL residue sequence from s0 = 4",
+                    "config": {"workload": f"LL q={q} n=2^{n.bit_length() - 1}", "plan": t.plan,
+                               "iterations": ips, "res64": f"{t.res64():016x}"},
+                    "kernels": {k: {"launches": v[0], "avg_us": v[1] * 1e3 / max(v[0], 1)}
+                                for k, v in prof.items()},
+                    "reference_build_us_per_iteration": ref.get(n)}
+        print(json.dumps(line), flush=True)
 
 
 def reference_plain_tests_per_hour(cuda_b200, exps, target_of):
@@ -436,6 +477,10 @@ def main():
     if args.workload == "c1":
         if rank == 0:
             run_c1(args)
+        return
+    if args.workload == "lengths":
+        if rank == 0:
+            run_lengths(args)
         return
     if args.workload in ("c3", "c4", "c5"):
         import random
