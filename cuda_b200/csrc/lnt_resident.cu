@@ -127,8 +127,24 @@ size_t resident_smem_bytes(uint32_t n, uint32_t threads) {
 cudaError_t launch_resident(const ResidentDesc* d_descs, uint32_t count, uint32_t max_n,
                             cudaStream_t stream) {
   const uint32_t threads = resident_threads(max_n, count);
-  const size_t smem = resident_smem_bytes(max_n, threads);
-  cudaError_t e = cudaFuncSetAttribute(resident_square_loop,
+  size_t smem = resident_smem_bytes(max_n, threads);
+  // Fewer tests than SMs: every test gets an SM of its own.  Left to itself
+  // the block scheduler may place two of the CTAs on one SM (their registers
+  // and shared memory fit), which halves both tests' speed while other SMs
+  // idle; a CTA holding more than half of an SM's shared memory cannot share.
+  int dev = 0, sms = 0, per_sm = 0, per_block = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess)
+    e = cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  if (e == cudaSuccess)
+    e = cudaDeviceGetAttribute(&per_block, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e != cudaSuccess) return e;
+  if (count > 1 && count <= (uint32_t)sms) {
+    const size_t solo = (size_t)per_sm / 2 + 1024;
+    if (solo > smem && solo <= (size_t)per_block) smem = solo;
+  }
+  e = cudaFuncSetAttribute(resident_square_loop,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   resident_square_loop<<<count, threads, smem, stream>>>(d_descs);
