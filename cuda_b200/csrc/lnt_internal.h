@@ -32,7 +32,7 @@ struct Plan {
   bool fast = false;    // register-pass kernels (lnt_radix16.cu) instead of radix-2
   // steady squarings use the carry-fused column kernel (col_inverse of one
   // squaring + col_forward of the next): from 2^19 words, where its tiles fill
-  // the GPU (at n = 2^23: 297 us for the pair that takes 308 us as two
+  // the GPU (at n = 2^23: 244.6 us for the pair that takes 270.1 us as two
   // launches); below, where a squaring is latency-bound, two plain launches win
   bool fused = false;
   std::string name;
