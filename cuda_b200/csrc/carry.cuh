@@ -46,4 +46,25 @@ GL_HD int64_t balance(int64_t t, unsigned w, int64_t& k) {
   return t - (k << w);
 }
 
+// A convolution output c plus the incoming carry, as one balanced digit (the
+// return value) and the outgoing carry (*out).  The same pair as split_output
+// followed by balance(lo + carry), with one balance of c + carry instead: with
+// c = hi 2^w + lo, floor((c + carry + 2^(w-1)) / 2^w) = hi + floor((lo + carry +
+// 2^(w-1)) / 2^w).  Signed outputs stay below p/4 in magnitude (the length
+// policy's bound), so c + carry cannot overflow; the unsigned reading of the
+// first squaring, up to p, keeps the split.
+GL_HD int64_t carry_digit(uint64_t c, bool unsigned_mode, int64_t carry, unsigned w, int64_t& out) {
+  int64_t q;
+  if (unsigned_mode) {
+    int64_t hi, lo;
+    split_output(c, true, w, hi, lo);
+    const int64_t d = balance(lo + carry, w, q);
+    out = hi + q;
+    return d;
+  }
+  const int64_t d = balance(gl::to_signed(c) + carry, w, q);
+  out = q;
+  return d;
+}
+
 }  // namespace lnt

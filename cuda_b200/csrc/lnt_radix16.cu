@@ -379,10 +379,7 @@ __device__ __forceinline__ void inverse_tile(const TwoPassDesc& D, const Passes&
 #pragma unroll
     for (int c = 0; c < T; ++c) {
       uint64_t& v = sm[c * ld + sw(r)];
-      int64_t hi, lo, q;
-      split_output(gl::mul(v, uw[c]), unsigned_mode, wd[c], hi, lo);
-      v = (uint64_t)balance(lo + carry, wd[c], q);
-      carry = hi + q;
+      v = (uint64_t)carry_digit(gl::mul(v, uw[c]), unsigned_mode, carry, wd[c], carry);
     }
     D.carry[run] = carry;
   }

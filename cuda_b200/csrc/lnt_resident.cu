@@ -82,11 +82,7 @@ __global__ void __launch_bounds__(kMaxThreads) resident_square_loop(const Reside
       int64_t carry = (!D.prp && tid == 0) ? -2 : 0;
       for (uint32_t k = 0; k < K; ++k) {
         const uint32_t j = tid * K + k;
-        int64_t hi, lo, q;
-        split_output(gl::mul(s[sw(j)], uw[j]), um, wd[j], hi, lo);
-        const int64_t d = balance(lo + carry, wd[j], q);
-        carry = hi + q;
-        s[sw(j)] = (uint64_t)d;
+        s[sw(j)] = (uint64_t)carry_digit(gl::mul(s[sw(j)], uw[j]), um, carry, wd[j], carry);
       }
       runc[tid] = carry;
     }

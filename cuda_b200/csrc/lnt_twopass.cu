@@ -176,10 +176,7 @@ __global__ void __launch_bounds__(kThreads) col_inverse(TwoPassDesc D, int unsig
     for (uint32_t c = 0; c < T; ++c) {
       uint64_t& v = sm[(size_t)c * ld + r];
       const unsigned w = D.widths[jrow + c];
-      int64_t hi, lo, q;
-      split_output(v, unsigned_mode != 0, w, hi, lo);
-      v = (uint64_t)balance(lo + carry, w, q);
-      carry = hi + q;
+      v = (uint64_t)carry_digit(v, unsigned_mode != 0, carry, w, carry);
     }
     D.carry[(size_t)t0 * n2 + r] = carry;
   }

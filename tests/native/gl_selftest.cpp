@@ -73,6 +73,21 @@ int main() {
       CHECK((__int128)hi * ((__int128)1 << w) + lo == s && lo >= 0 && lo < (int64_t(1) << w),
             "split signed %llx w=%u", (unsigned long long)c, w);
     }
+  // carry_digit = split_output then balance(lo + carry), both readings; signed
+  // outputs within the p/4 bound, carries of either sign
+  for (unsigned w = 1; w <= 30; ++w)
+    for (int i = 0; i < 4000; ++i) {
+      const bool um = (i & 1) != 0;
+      uint64_t c = rng() % gl::P;
+      if (!um) c = gl::from_signed((int64_t)(rng() >> 3) - (int64_t)(1ull << 60));  // |s| < 2^61
+      const int64_t carry = (int64_t)(rng() >> 28) - (int64_t)(1ull << 35);
+      int64_t hi, lo, q, out;
+      lnt::split_output(c, um, w, hi, lo);
+      const int64_t d0 = lnt::balance(lo + carry, w, q);
+      const int64_t d1 = lnt::carry_digit(c, um, carry, w, out);
+      CHECK(d1 == d0 && out == hi + q, "carry_digit %llx carry=%lld w=%u um=%d", (unsigned long long)c,
+            (long long)carry, w, (int)um);
+    }
   if (fails) { std::printf("FAILED %d of %ld\n", fails, cases); return 1; }
   std::printf("ok %ld\n", cases);
   return 0;
