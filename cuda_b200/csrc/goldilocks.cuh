@@ -14,6 +14,10 @@
 #ifndef LNT_GL_SHORT
 #define LNT_GL_SHORT 1
 #endif
+// LNT_GL_SUBMAD = 1: the borrow correction of sub_chain on the multiplier pipe.
+#ifndef LNT_GL_SUBMAD
+#define LNT_GL_SUBMAD 1
+#endif
 
 #if defined(__CUDACC__)
 #define GL_HD __host__ __device__ __forceinline__
@@ -40,7 +44,23 @@ GL_HD uint64_t mulhi(uint64_t a, uint64_t b) {
 // selects the correction (+p: low word + 1, high word + 2^32 - 1), no compare.
 __device__ __forceinline__ uint64_t sub_chain(uint32_t a0, uint32_t a1, uint32_t b0, uint32_t b1) {
   uint32_t d0, d1;
-#if LNT_GL_SHORT
+#if LNT_GL_SUBMAD
+  // the wrapped difference plus p times the borrow b, with the borrow mask
+  // m = -b: its low word gains m * m = b (mod 2^32) on the multiplier pipe (m is
+  // not a constant, so the multiply stays a multiply), its high word m plus the
+  // carry.  Same result and instruction count as the two subtractions below,
+  // one of them moved off the integer ALU pipe.
+  asm("{\n\t"
+      ".reg .u32 m;\n\t"
+      "sub.cc.u32    %0, %2, %4;\n\t"
+      "subc.cc.u32   %1, %3, %5;\n\t"
+      "subc.u32      m, 0, 0;\n\t"
+      "mad.lo.cc.u32 %0, m, m, %0;\n\t"
+      "addc.u32      %1, %1, m;\n\t"
+      "}"
+      : "=r"(d0), "=r"(d1)
+      : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
+#elif LNT_GL_SHORT
   // the wrapped difference minus 2^64 - p = 2^32 - 1, which is the borrow mask
   asm("{\n\t"
       ".reg .u32 m;\n\t"
