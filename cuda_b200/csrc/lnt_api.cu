@@ -419,6 +419,7 @@ int queue_iterations(lnt_test* t, uint64_t iterations, LaunchTimer* timer) {
     d.prp = (uint32_t)t->prp;
     d.unsigned_first = t->canonical_input ? 1 : 0;
     d.iterations = iterations;
+    d.short_runs = lnt::r16_run_words_needed(t->q, t->plan.log2n) <= 4 ? 1 : 0;
     LNT_CUDA(cudaMemcpyAsync(t->rdesc, &d, sizeof(d), cudaMemcpyHostToDevice, t->stream),
              "upload descriptor");
     LNT_LAUNCH(lnt::launch_resident(t->rdesc, 1, t->n, t->stream), "resident_square_loop");
@@ -737,6 +738,7 @@ ResidentDesc test_resident_desc(const lnt_test* t, uint64_t iterations) {
   d.prp = (uint32_t)t->prp;
   d.unsigned_first = t->canonical_input ? 1 : 0;
   d.iterations = iterations;
+  d.short_runs = r16_run_words_needed(t->q, t->plan.log2n) <= 4 ? 1 : 0;
   return d;
 }
 // bookkeeping after squarings were launched outside lnt_iterate

@@ -71,6 +71,7 @@ struct ResidentDesc {
   uint32_t prp;
   uint32_t unsigned_first;  // the first squaring reads its outputs as non-negative
   uint64_t iterations;      // squarings this CTA performs in the launch
+  uint32_t short_runs;      // carry runs of 4 words suffice for this exponent (else 8)
 };
 
 size_t resident_smem_bytes(uint32_t n, uint32_t threads);

@@ -30,7 +30,8 @@ constexpr uint32_t kMaxThreads = 1024;
 // SMs, where latency, not throughput, decides (n = 2048 alone: 11.9 us per
 // squaring with 512 threads, 12.9 with 256; nine tests: 48K vs 55K tests/hour).
 
-__global__ void __launch_bounds__(kMaxThreads) resident_square_loop(const ResidentDesc* descs) {
+__global__ void __launch_bounds__(kMaxThreads) resident_square_loop(const ResidentDesc* descs,
+                                                                    int latency_mode) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const ResidentDesc D = descs[blockIdx.x];
   const uint32_t n = D.n;
@@ -43,8 +44,11 @@ __global__ void __launch_bounds__(kMaxThreads) resident_square_loop(const Reside
   uint8_t* wd = reinterpret_cast<uint8_t*>(runc + bd);
   const Passes P = make_passes((int)D.log2n);
 
-  const uint32_t runs = n >= kRunWords ? n / kRunWords : 1;  // active carry threads
-  const uint32_t K = n / runs;                              // words per run
+  // latency mode: runs of 4 words where the exponent allows, one per thread
+  // (n / 4 threads), which halves each thread's carry chain
+  const uint32_t run_words = latency_mode && D.short_runs ? 4u : kRunWords;
+  const uint32_t runs = n >= run_words ? n / run_words : 1;  // active carry threads
+  const uint32_t K = n / runs;                               // words per run
 
   for (uint32_t j = tid; j < n; j += bd) {
     s[sw(j)] = (uint64_t)D.digits[j];
@@ -143,7 +147,7 @@ cudaError_t launch_resident(const ResidentDesc* d_descs, uint32_t count, uint32_
   e = cudaFuncSetAttribute(resident_square_loop,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  resident_square_loop<<<count, threads, smem, stream>>>(d_descs);
+  resident_square_loop<<<count, threads, smem, stream>>>(d_descs, count < 148 ? 1 : 0);
   return cudaGetLastError();
 }
 
