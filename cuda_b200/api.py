@@ -111,6 +111,7 @@ def lib() -> ctypes.CDLL:
         "lnt_gerbicz_enable": ([vp, u32], i32),
         "lnt_gerbicz_stats": ([vp, ctypes.POINTER(u64), ctypes.POINTER(u64), ctypes.POINTER(u64)], i32),
         "lnt_debug_corrupt": ([vp, u32], i32),
+        "lnt_debug_corrupt_add": ([vp, u32, ctypes.c_int64], i32),
         "lnt_batch_use_graphs": ([vp, i32], i32),
         "lnt_arith_selftest": ([i32, ctypes.POINTER(u64), ctypes.POINTER(u64)], i32),
     }
@@ -282,9 +283,10 @@ class LucasTest:
                "lnt_gerbicz_stats")
         return {"verified_iterations": int(v.value), "checks": int(c.value), "errors": int(e.value)}
 
-    def debug_corrupt(self, word: int = 1) -> None:
-        """Test hook: add 1 to one word of the device state (a simulated hardware error)."""
-        _check(lib().lnt_debug_corrupt(self._h, int(word)), "lnt_debug_corrupt")
+    def debug_corrupt(self, word: int = 1, delta: int = 1) -> None:
+        """Test hook: add `delta` to one word of the device state (a simulated
+        hardware error; a large delta makes the kernels raise the carry flag)."""
+        _check(lib().lnt_debug_corrupt_add(self._h, int(word), int(delta)), "lnt_debug_corrupt_add")
 
     def set_stream(self, stream_handle: int | None) -> None:
         _check(lib().lnt_set_stream(self._h, stream_handle), "lnt_set_stream")

@@ -513,6 +513,7 @@ struct Gerbicz {
   StateBuf f;                        // scratch: the transformed operand of a product
   TwoPassDesc* fdesc = nullptr;      // device descriptor of `f`
   uint64_t done = 0, verified = 0, checks = 0, errors = 0;
+  uint32_t failed_in_a_row = 0;  // recoveries since the last passed verification
   bool have_prev = false;
 };
 
@@ -644,6 +645,36 @@ int square_state(lnt_test* t, lnt::StateBuf& s, uint64_t k) {
   return st != LNT_OK ? st : st2;
 }
 
+// Recoveries in a row without a passed verification before the error is
+// returned: a fault that repeats on the same squarings is not transient.
+constexpr uint32_t kGerbiczRetries = 3;
+
+// The kernels' status word (sticky bits, lnt::kStatus*), read on the stream.
+int read_status(lnt_test* t, uint32_t& flags) {
+  LNT_CUDA(cudaMemcpyAsync(t->h_pinned, t->status, 4, cudaMemcpyDeviceToHost, t->stream), "read status");
+  LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
+  flags = t->h_pinned[0];
+  return LNT_OK;
+}
+
+// A detected error (a failed comparison, or a carry that left the
+// balanced-digit headroom, which only corrupted data produces): back to the
+// last verified residue and product, with the carry flag cleared.
+int gerbicz_recover(lnt_test* t) {
+  lnt::Gerbicz& g = *t->gz;
+  ++g.errors;
+  if (++g.failed_in_a_row > kGerbiczRetries)
+    return fail(LNT_ERR_NUMERIC, "Gerbicz check: the same squarings failed " +
+                                     std::to_string(kGerbiczRetries) + " times in a row");
+  int st;
+  if ((st = load_main(t, g.xok)) != LNT_OK || (st = copy_state(t, g.d, g.dok)) != LNT_OK) return st;
+  LNT_CUDA(cudaMemsetAsync(t->status, 0, 4, t->stream), "clear status");
+  LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
+  g.done = g.verified;
+  g.have_prev = false;
+  return LNT_OK;
+}
+
 // Start (or restart) the chain at the test's current residue.
 int gerbicz_rebase(lnt_test* t) {
   lnt::Gerbicz& g = *t->gz;
@@ -651,6 +682,7 @@ int gerbicz_rebase(lnt_test* t) {
   for (lnt::StateBuf* s : {&g.c0, &g.d, &g.xok, &g.dok})
     if ((st = save_main(t, *s)) != LNT_OK) return st;
   g.done = g.verified = 0;
+  g.failed_in_a_row = 0;
   g.have_prev = false;
   return LNT_OK;
 }
@@ -663,48 +695,75 @@ int gerbicz_verify(lnt_test* t, bool& ok) {
   if ((st = copy_state(t, g.v, g.dprev)) != LNT_OK) return st;
   if ((st = square_state(t, g.v, g.block)) != LNT_OK) return st;
   if ((st = mul_state(t, g.v, g.c0)) != LNT_OK) return st;
-  std::vector<uint64_t> lhs, rhs;
-  if ((st = state_digits(t, g.d, lhs)) != LNT_OK) return st;
-  if ((st = state_digits(t, g.v, rhs)) != LNT_OK) return st;
-  ok = lhs == rhs;
+  // a carry flagged anywhere since the last look fails the check without a readout
+  uint32_t flags = 0;
+  if ((st = read_status(t, flags)) != LNT_OK) return st;
+  ok = false;
+  if (!(flags & lnt::kStatusCarryOverflow)) {
+    std::vector<uint64_t> lhs, rhs;
+    if ((st = state_digits(t, g.d, lhs)) != LNT_OK) return st;
+    if ((st = state_digits(t, g.v, rhs)) != LNT_OK) return st;
+    ok = lhs == rhs;
+  }
   if (ok) {
     if ((st = save_main(t, g.xok)) != LNT_OK || (st = copy_state(t, g.dok, g.d)) != LNT_OK) return st;
     g.verified = g.done;
+    g.failed_in_a_row = 0;
     ++g.checks;
-  } else {
-    ++g.errors;
-    if ((st = load_main(t, g.xok)) != LNT_OK || (st = copy_state(t, g.d, g.dok)) != LNT_OK) return st;
-    g.done = g.verified;
-    g.have_prev = false;
+  } else if ((st = gerbicz_recover(t)) != LNT_OK) {
+    return st;
   }
   LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
   return LNT_OK;
 }
 
+// A carry flagged by the kernels since the last look: recover (and redo the
+// squarings since the last verification).  Called where the stream is about to
+// be drained anyway.
+int gerbicz_check_carries(lnt_test* t, uint64_t& left, bool& recovered) {
+  lnt::Gerbicz& g = *t->gz;
+  uint32_t flags = 0;
+  int st = read_status(t, flags);
+  recovered = false;
+  if (st != LNT_OK || !(flags & lnt::kStatusCarryOverflow)) return st;
+  const uint64_t before = g.done;
+  if ((st = gerbicz_recover(t)) != LNT_OK) return st;
+  left += before - g.done;
+  recovered = true;
+  return LNT_OK;
+}
+
 // lnt_iterate with the check: `iterations` squarings that are (up to the last
-// B^2 boundary) verified, redoing blocks that fail.
+// B^2 boundary) verified, redoing blocks that fail a comparison or raise the
+// carry flag.
 int gerbicz_iterate(lnt_test* t, uint64_t iterations) {
   lnt::Gerbicz& g = *t->gz;
   const uint64_t B = g.block;
   uint64_t left = iterations;
-  while (left) {
-    const uint64_t step = std::min<uint64_t>(left, B - g.done % B);
-    int st = queue_iterations(t, step, nullptr);
-    if (st != LNT_OK) return st;
-    g.done += step;
-    left -= step;
-    if (g.done % B != 0) continue;
-    // checkpoint: D_{k-1} kept, D_k = D_{k-1} * x
-    lnt::StateBuf x = main_state(t);
-    if ((st = copy_state(t, g.dprev, g.d)) != LNT_OK) return st;
-    if ((st = mul_state(t, g.d, x)) != LNT_OK) return st;
-    g.have_prev = true;
-    if ((g.done / B) % B == 0) {
-      const uint64_t before = g.done;
-      bool ok = false;
-      if ((st = gerbicz_verify(t, ok)) != LNT_OK) return st;
-      if (!ok) left += before - g.done;  // redo what the failed block covered
+  int st;
+  for (bool recovered = true; recovered;) {
+    while (left) {
+      const uint64_t step = std::min<uint64_t>(left, B - g.done % B);
+      if ((st = queue_iterations(t, step, nullptr)) != LNT_OK) return st;
+      g.done += step;
+      left -= step;
+      if (g.done % B != 0) continue;
+      if ((st = gerbicz_check_carries(t, left, recovered)) != LNT_OK) return st;
+      if (recovered) continue;
+      // checkpoint: D_{k-1} kept, D_k = D_{k-1} * x
+      lnt::StateBuf x = main_state(t);
+      if ((st = copy_state(t, g.dprev, g.d)) != LNT_OK) return st;
+      if ((st = mul_state(t, g.d, x)) != LNT_OK) return st;
+      g.have_prev = true;
+      if ((g.done / B) % B == 0) {
+        const uint64_t before = g.done;
+        bool ok = false;
+        if ((st = gerbicz_verify(t, ok)) != LNT_OK) return st;
+        if (!ok) left += before - g.done;  // redo what the failed block covered
+      }
     }
+    // no carry flag may reach the caller: a last look, and a redo if needed
+    if ((st = gerbicz_check_carries(t, left, recovered)) != LNT_OK) return st;
   }
   return LNT_OK;
 }
@@ -961,13 +1020,15 @@ int lnt_gerbicz_stats(lnt_test* t, uint64_t* verified_iterations, uint64_t* chec
   return LNT_OK;
 }
 
-int lnt_debug_corrupt(lnt_test* t, uint32_t word) {
+int lnt_debug_corrupt(lnt_test* t, uint32_t word) { return lnt_debug_corrupt_add(t, word, 1); }
+
+int lnt_debug_corrupt_add(lnt_test* t, uint32_t word, int64_t delta) {
   if (!t || word >= t->n) return fail(LNT_ERR_INVALID_ARGUMENT, "word out of range");
   DeviceGuard guard(t->device);
   LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
   int64_t v = 0;
   LNT_CUDA(cudaMemcpy(&v, t->x + word, 8, cudaMemcpyDeviceToHost), "read word");
-  v += 1;
+  v += delta;
   LNT_CUDA(cudaMemcpy(t->x + word, &v, 8, cudaMemcpyHostToDevice), "write word");
   t->canon_valid = false;
   return LNT_OK;

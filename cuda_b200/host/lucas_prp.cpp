@@ -139,8 +139,13 @@ void LucasPRP::MainLoop() {
     }
     const uint64_t todo = std::min({(uint64_t)o_.iterations - cur + 1, chunk, dump_every - since_dump,
                                     pit_stop - since_pit});
-    Check(lnt_iterate(t_, todo), "lnt_iterate");
-    Check(lnt_synchronize(t_), "lnt_synchronize");
+    int st = lnt_iterate(t_, todo);
+    if (st == LNT_OK) st = lnt_synchronize(t_);
+    if (st != LNT_OK) {
+      // which squarings failed, for the user's report
+      const std::string where = "squarings " + std::to_string(cur) + " to " + std::to_string(cur + todo - 1);
+      Check(st, where.c_str());
+    }
     cur += todo;
     since_dump += todo;
     since_pit += todo;

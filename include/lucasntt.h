@@ -157,9 +157,12 @@ int lnt_is_prime(lnt_test* t, int* is_prime);
  * (lucas_prp.cu:137-195).  For PRP tests on two-pass plans (n >= 8192):
  * every `block` squarings lnt_iterate folds the residue into a running
  * product D of checkpoint residues, and every block^2 squarings it verifies
- * D_k = x_0 * D_{k-1}^(2^block); on a mismatch it returns to the last verified
- * residue and redoes the work, so the residues it returns are the error-free
- * ones up to the last verification.  Costs about 2.5 squarings per block plus
+ * D_k = x_0 * D_{k-1}^(2^block); on a mismatch, or when the kernels flag a
+ * carry outside the balanced-digit headroom (which only corrupted data
+ * produces), it returns to the last verified residue and redoes the work, so
+ * the residues it returns are the error-free ones up to the last verification.
+ * After 3 such recoveries in a row without a passed verification it returns
+ * LNT_ERR_NUMERIC: the fault is not transient.  Costs about 2.5 squarings per block plus
  * `block` per block^2 (under 0.5 % at block = 1000) and 7 residue-sized
  * buffers.  lnt_set_digits / lnt_init_test restart the chain.
  * block = 0 turns the check off.  LNT_ERR_INVALID_ARGUMENT for LL tests,
@@ -173,6 +176,10 @@ int lnt_gerbicz_stats(lnt_test* t, uint64_t* verified_iterations, uint64_t* chec
 /* Diagnostic without a reference counterpart, for tests of the check: adds 1
  * to word `word` of the device state, as a hardware error would corrupt it. */
 int lnt_debug_corrupt(lnt_test* t, uint32_t word);
+
+/* The same with any amount: a large `delta` (say 2^40) makes the next squarings
+ * raise the kernels' carry flag, which the check also treats as an error. */
+int lnt_debug_corrupt_add(lnt_test* t, uint32_t word, int64_t delta);
 
 /* Length, widths (n bytes, pre_calculation.cu:35) and plan name of a test. */
 int lnt_get_length(lnt_test* t, uint32_t* n);

@@ -5,7 +5,8 @@ it is exercised end to end: a checked PRP test of a Mersenne prime still ends
 with residue 9; a checked test gives the same residue as an unchecked one; and
 a residue word corrupted between calls (what a hardware error would do) is
 detected at the next verification and the test recovers to the error-free
-residue.
+residue; a corruption large enough to make the kernels raise the carry flag is
+recovered the same way instead of failing the call.
 """
 import pytest
 
@@ -68,3 +69,18 @@ def test_check_needs_prp_and_a_two_pass_plan(lnt):
     with lnt.LucasTest(9941, prp=True) as t:  # n = 512: SMEM-resident plan
         with pytest.raises(lnt.LucasNTTError):
             t.gerbicz_enable(64)
+
+
+@pytest.mark.parametrize("at", [4992, 5009])  # on a block boundary, inside a block
+def test_carry_flag_from_a_corrupted_word_is_recovered(lnt, at):
+    q, block, iterations = 160001, 32, 12000
+    with lnt.LucasTest(q, prp=True) as t:
+        t.gerbicz_enable(block)
+        t.iterate(at)
+        t.debug_corrupt(17, 1 << 40)  # far outside the balanced-digit range
+        t.iterate(iterations - at)
+        t.synchronize()
+        st = t.gerbicz_stats()
+        assert st["errors"] >= 1
+        assert st["checks"] == iterations // (block * block)
+        assert t.res64() == plain_res64(lnt, q, iterations)
