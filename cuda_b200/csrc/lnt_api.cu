@@ -177,8 +177,12 @@ int upload_roots(lnt_test* t, uint32_t n, uint64_t** rt, uint64_t** irt, bool fu
   }
   LNT_CUDA(dalloc(rt, a.size()), "cudaMalloc roots");
   LNT_CUDA(dalloc(irt, b.size()), "cudaMalloc roots");
-  LNT_CUDA(cudaMemcpy(*rt, a.data(), a.size() * 8, cudaMemcpyHostToDevice), "copy roots");
-  LNT_CUDA(cudaMemcpy(*irt, b.data(), b.size() * 8, cudaMemcpyHostToDevice), "copy roots");
+  // host-to-device copies go on the test's (non-blocking) stream, ahead of the
+  // kernels that read them: a plain cudaMemcpy from pageable memory may return
+  // before its DMA lands, and it is not ordered with work on that stream
+  LNT_CUDA(cudaMemcpyAsync(*rt, a.data(), a.size() * 8, cudaMemcpyHostToDevice, t->stream), "copy roots");
+  LNT_CUDA(cudaMemcpyAsync(*irt, b.data(), b.size() * 8, cudaMemcpyHostToDevice, t->stream), "copy roots");
+  LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
   return LNT_OK;
 }
 
@@ -315,8 +319,9 @@ int canonicalize(lnt_test* t) {
     std::vector<uint64_t> out;
     canonicalize_host(x, carries, t, out);
     fix_zero_representation(t, out);
-    LNT_CUDA(cudaMemcpy(t->canon, out.data(), (size_t)t->n * 8, cudaMemcpyHostToDevice),
+    LNT_CUDA(cudaMemcpyAsync(t->canon, out.data(), (size_t)t->n * 8, cudaMemcpyHostToDevice, t->stream),
              "upload digits");
+    LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
     t->canon_valid = true;
     return LNT_OK;
   }
@@ -563,7 +568,9 @@ int swap_state(lnt_test* t, lnt::StateBuf& s) {
   std::swap(t->zero_start, s.zero_start);
   t->canon_valid = false;
   const lnt::TwoPassDesc hd = twopass_desc(t);
-  LNT_CUDA(cudaMemcpy(t->tdesc, &hd, sizeof(hd), cudaMemcpyHostToDevice), "descriptor");
+  // on the test's stream, so the next kernel cannot read the previous state's descriptor
+  LNT_CUDA(cudaMemcpyAsync(t->tdesc, &hd, sizeof(hd), cudaMemcpyHostToDevice, t->stream), "descriptor");
+  LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
   return LNT_OK;
 }
 
@@ -601,7 +608,8 @@ int mul_state(lnt_test* t, lnt::StateBuf& a, const lnt::StateBuf& b) {
   fd.x = g.f.x;
   fd.carry = g.f.carry;
   LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
-  LNT_CUDA(cudaMemcpy(g.fdesc, &fd, sizeof(fd), cudaMemcpyHostToDevice), "descriptor");
+  LNT_CUDA(cudaMemcpyAsync(g.fdesc, &fd, sizeof(fd), cudaMemcpyHostToDevice, t->stream), "descriptor");
+  LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
   // the operand's full transform, in place in f
   LNT_CUDA(lnt::launch_col_forward_r16(geo, g.fdesc, 1, b.pending_carries, t->stream), "col_forward");
   LNT_CUDA(lnt::launch_row_forward_r16(geo, g.fdesc, t->stream), "row_forward");
@@ -903,8 +911,8 @@ int lnt_create_with_plan(uint32_t exponent, uint32_t n, int prp, int device,
       (e = dalloc(&t->blk_cin, nb)) || (e = dalloc(&t->cflags, 1)) ||
       (e = cudaMallocHost((void**)&t->h_pinned, 16)))
     return bail(cuda_fail(e, "allocate residue"));
-  if ((e = cudaMemcpy(t->widths, t->h_widths.data(), n, cudaMemcpyHostToDevice)) ||
-      (e = cudaMemset(t->status, 0, 4)))
+  if ((e = cudaMemcpyAsync(t->widths, t->h_widths.data(), n, cudaMemcpyHostToDevice, t->stream)) ||
+      (e = cudaMemsetAsync(t->status, 0, 4, t->stream)))
     return bail(cuda_fail(e, "upload widths"));
   if ((e = lnt::launch_weights(exponent, n, t->w, t->uw, t->stream)))
     return bail(cuda_fail(e, "weights"));
@@ -927,7 +935,7 @@ int lnt_create_with_plan(uint32_t exponent, uint32_t n, int prp, int device,
     if ((e = dalloc(&t->twf, n)) || (e = dalloc(&t->twi, n)) ||
         (e = dalloc(&t->carry, (size_t)plan.ntiles * plan.n2)) ||
         (e = dalloc(&t->fuse, (size_t)plan.ntiles + 2)) ||
-        (e = cudaMemset(t->fuse, 0, ((size_t)plan.ntiles + 2) * 4)))
+        (e = cudaMemsetAsync(t->fuse, 0, ((size_t)plan.ntiles + 2) * 4, t->stream)))
       return bail(cuda_fail(e, "allocate twiddles"));
     if ((e = lnt::launch_twiddles(plan.n1, plan.n2, plan.log2n2, t->twf, t->twi, t->stream)))
       return bail(cuda_fail(e, "twiddles"));
@@ -940,7 +948,8 @@ int lnt_create_with_plan(uint32_t exponent, uint32_t n, int prp, int device,
     if (plan.fast && (!hd.itw1 || !hd.iitw1 || !hd.itw2 || !hd.iitw2 || !hd.wt || !hd.uwt || !hd.widt))
       return bail(fail(LNT_ERR_CUDA, "internal: descriptor built before its buffers"));
     if ((e = dalloc(&t->tdesc, 1)) ||
-        (e = cudaMemcpy(t->tdesc, &hd, sizeof(hd), cudaMemcpyHostToDevice)))
+        (e = cudaMemcpyAsync(t->tdesc, &hd, sizeof(hd), cudaMemcpyHostToDevice, t->stream)) ||
+        (e = cudaStreamSynchronize(t->stream)))
       return bail(cuda_fail(e, "descriptor"));
   }
   if ((e = cudaStreamSynchronize(t->stream))) return bail(cuda_fail(e, "initialize"));
@@ -1029,7 +1038,8 @@ int lnt_debug_corrupt_add(lnt_test* t, uint32_t word, int64_t delta) {
   int64_t v = 0;
   LNT_CUDA(cudaMemcpy(&v, t->x + word, 8, cudaMemcpyDeviceToHost), "read word");
   v += delta;
-  LNT_CUDA(cudaMemcpy(t->x + word, &v, 8, cudaMemcpyHostToDevice), "write word");
+  LNT_CUDA(cudaMemcpyAsync(t->x + word, &v, 8, cudaMemcpyHostToDevice, t->stream), "write word");
+  LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
   t->canon_valid = false;
   return LNT_OK;
 }

@@ -226,6 +226,9 @@ int rebuild(lnt_batch* b) {
     g.cap = h.size();
     BCUDA(cudaMemcpy(g.d_descs, h.data(), h.size() * sizeof(lnt::TwoPassDesc), cudaMemcpyHostToDevice),
           "upload descriptors");
+    // a copy from pageable memory may return before its DMA lands, and the
+    // group's kernels run on non-blocking streams that do not wait for it
+    BCUDA(cudaDeviceSynchronize(), "synchronize");
     g.stream = take_stream(b);
     BCUDA(cudaEventCreateWithFlags(&g.join, cudaEventDisableTiming), "group event");
   }
