@@ -5,7 +5,14 @@ Test infrastructure: pins residues against the reference build and measures its
 "Per iteration (ms)" (lucas_prp.cu:319).  Usage (on a GPU box):
 
   python oracle/run_ref.py --exponent Q --iterations K [--fft N] [--prp]
-                           [--loops 500] --out gpurun_out/ref_<tag>
+                           [--loops 500] --out OUTDIR
+  python oracle/run_ref.py --cases CASES.json [--loops 500] --out OUTDIR
+
+CASES.json is a list of {"q", "iterations", "prp", "fft"} objects (written by
+tests/golden/make_golden.py refcases); the cases run one after another and a
+case whose summary already exists in OUTDIR is skipped, so an interrupted list
+can be resumed.  Only the dumps' Res64 and SHA-256 are kept in this mode.
+tests/golden/make_golden.py ref OUTDIR collects the summaries.
 
 The program reads LucasNTT.ini from its working directory (main_process.cu:72)
 and takes `exponent iterations fileprefix fft` on the command line
@@ -42,7 +49,7 @@ def summarize_dump(dat: Path, exponent: int, n: int):
 
 
 def run(exponent: int, iterations: int, out: Path, fft: str | None = None, prp: bool = False,
-        loops: int = 500, timeout: int = 1800) -> dict:
+        loops: int = 500, timeout: int = 1800, keep_dump_bytes: int = 1 << 20) -> dict:
     out.mkdir(parents=True, exist_ok=True)
     (out / "LucasNTT.ini").write_text(
         "Verbosity = Normal\n"
@@ -69,7 +76,7 @@ def run(exponent: int, iterations: int, out: Path, fft: str | None = None, prp: 
     res64, words, digest = None, 0, None
     if dat.exists() and n:
         res64, words, digest = summarize_dump(dat, exponent, n)
-        if dat.stat().st_size > (1 << 20):
+        if dat.stat().st_size > keep_dump_bytes:
             dat.unlink()  # large dumps stay on the box; their Res64 and digest are kept
         else:
             dat.rename(out / f"{exponent}_{n}_{int(prp)}_{iterations}.dat")
@@ -83,14 +90,31 @@ def run(exponent: int, iterations: int, out: Path, fft: str | None = None, prp: 
     return res
 
 
+def run_cases(cases_file: Path, out: Path, loops: int) -> None:
+    cases = json.loads(cases_file.read_text())
+    t0 = time.time()
+    for i, c in enumerate(cases):
+        q, prp = int(c["q"]), bool(c["prp"])
+        it = int(c.get("iterations") or (q if prp else q - 2))
+        if (out / f"run_{q}_{it}_{int(prp)}.json").exists():
+            continue
+        r = run(q, it, out, c.get("fft"), prp, loops, keep_dump_bytes=0)
+        print(f"[{i + 1}/{len(cases)} {time.time() - t0:.0f}s] q={q} it={it} prp={int(prp)} n={r['n']} "
+              f"rc={r['rc']} res64={r['res64']} wall={r['wall_s']:.1f}s", flush=True)
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--exponent", type=int, required=True)
+    ap.add_argument("--cases")
+    ap.add_argument("--exponent", type=int)
     ap.add_argument("--iterations", type=int, default=0)
     ap.add_argument("--fft")
     ap.add_argument("--prp", action="store_true")
     ap.add_argument("--loops", type=int, default=500)
     ap.add_argument("--out", required=True)
     a = ap.parse_args()
+    if a.cases:
+        run_cases(Path(a.cases), Path(a.out), a.loops)
+        raise SystemExit(0)
     it = a.iterations or (a.exponent if a.prp else a.exponent - 2)
     print(json.dumps(run(a.exponent, it, Path(a.out), a.fft, a.prp, a.loops)))

@@ -10,8 +10,14 @@ Sets:
          from the C oracle
   c2     q = 139000003 (first prime above 1.39e8) at n = 2^23: Res64 after 1000
          iterations (and 10000 with --c2-long) from the C oracle
-  ref    parse the reference build's residue dumps collected on a B200
-         (gpurun_out/ref_*/) into ref_residues.json
+  refcases  write ref_cases.json, the list of reference-build runs that pin
+         PRP mode and the batch/serving exponents (run on a B200 by
+         oracle/run_ref.py --cases tests/golden/ref_cases.json --out DIR)
+  ref DIR...  merge the reference build's run summaries found in the given
+         directories (run_*.json written by oracle/run_ref.py) into
+         ref_residues.json (cases already there are kept)
+  reftimes DIR...  the reference build's per-iteration times from the same
+         summaries into ref_timings.json
 
 Every fixture records how it was made.  The oracle and the model are test
 infrastructure; see oracle/lnt_oracle.c for what they restate.
@@ -33,6 +39,47 @@ HERE = Path(__file__).resolve().parent
 
 C1_EXPONENTS = [44497, 44501, 44507, 44519, 44531, 44533, 44537, 44543, 44549]
 C2_EXPONENT = 139000003
+
+
+def primes_between(lo: int, hi: int) -> list[int]:
+    import numpy as np
+
+    sieve = np.ones(hi + 1, dtype=bool)
+    sieve[:2] = False
+    for k in range(2, int(hi ** 0.5) + 1):
+        if sieve[k]:
+            sieve[k * k::k] = False
+    return [int(x) for x in np.nonzero(sieve)[0] if x >= lo]
+
+
+def c3_exponents() -> list[int]:
+    """256 primes in [1e5, 2e6], random.Random(0).sample (the C3 batch)."""
+    import random
+
+    return random.Random(0).sample(primes_between(100000, 2000000), 256)
+
+
+def c4_exponents() -> list[int]:
+    """64 primes in [5e6, 2e7], random.Random(1).sample (the C4 PRP batch)."""
+    import random
+
+    return random.Random(1).sample(primes_between(5000000, 20000000), 64)
+
+
+def c5_pool(lo: int = 10000, hi: int = 30000000, count: int = 64) -> list[tuple[int, bool]]:
+    """The serving stream's request pool: `count` draws of (q, prp), q the
+    smallest prime >= exp(U(ln lo, ln hi)), prp by a fair coin, random.Random(2)."""
+    import bisect
+    import math
+    import random
+
+    primes = primes_between(lo, hi + 100000)
+    rng = random.Random(2)
+    out = []
+    for _ in range(count):
+        x = math.exp(rng.uniform(math.log(lo), math.log(hi)))
+        out.append((primes[min(bisect.bisect_left(primes, int(x)), len(primes) - 1)], rng.random() < 0.5))
+    return out
 
 
 def is_prime(k: int) -> bool:
@@ -101,38 +148,92 @@ def make_c2(long_run: bool) -> None:
                  "n": 1 << 23, "res64_after": res})
 
 
-def make_ref() -> None:
-    """Collect the reference runs summarised by oracle/run_ref.py on a B200
-    (gpurun_out/ref_*/run_*.json: Res64 of its LucasNTT_results.dat dump)."""
-    base = ROOT / "gpurun_out"
-    cases = []
-    for js in sorted(base.glob("ref_*/run_*.json")):
-        r = json.loads(js.read_text())
-        if r.get("rc") != 0 or not r.get("res64"):
-            continue
-        cases.append({"q": r["exponent"], "n": r["n"], "prp": r["prp"], "iterations": r["iterations"],
-                      "res64": r["res64"], "fft": r["fft_used"], "pool": r["pool"],
-                      "per_iteration_ms": r["per_iteration_ms"], "conclusion": r["conclusion"],
-                      "dump_sha256": r.get("sha256_of_dump")})
+C3_CHECK_ITERATIONS = 20000
+C4_ITERATIONS = 20000
+C5_FULL_LIMIT = 610000
+
+
+def ref_cases() -> list[dict]:
+    """Reference-build runs pinning PRP mode and the batch and serving exponents.
+
+    C4: all 64 PRP tests at 20,000 squarings.  C3: a full LL test of the first
+    sampled exponent of each length, and every one of the 256 exponents after
+    20,000 squarings.  PRP: full tests of a composite and of Mersenne primes on
+    both plan kinds, and q = 139000003 after 1,000 squarings.  C5: full tests of
+    the pool's requests up to q = 610,000."""
+    from oracle import oracle as O
+
+    cases = [{"q": q, "iterations": C4_ITERATIONS, "prp": True, "set": "c4"} for q in c4_exponents()]
+    first = {}
+    for q in c3_exponents():
+        first.setdefault(1 << O.secured_log2(q), q)
+    cases += [{"q": q, "iterations": q - 2, "prp": False, "set": "c3_full"} for _, q in sorted(first.items())]
+    cases += [{"q": 100003, "iterations": 100003, "prp": True, "set": "prp"},
+              {"q": 160001, "iterations": 160001, "prp": True, "set": "prp"},
+              {"q": 132049, "iterations": 132049, "prp": True, "set": "prp"},
+              {"q": 44497, "iterations": 44497, "prp": True, "set": "prp"},
+              {"q": 44497, "iterations": 44497, "prp": True, "fft": "4096", "set": "prp"},
+              {"q": 44501, "iterations": 44501, "prp": True, "set": "prp"},
+              {"q": C2_EXPONENT, "iterations": 1000, "prp": True, "set": "prp"}]
+    seen = set()
+    for q, prp in sorted(c5_pool()):
+        if q <= C5_FULL_LIMIT and (q, prp) not in seen:
+            seen.add((q, prp))
+            cases.append({"q": q, "iterations": q if prp else q - 2, "prp": prp, "set": "c5_full"})
+    cases += [{"q": q, "iterations": C3_CHECK_ITERATIONS, "prp": False, "set": "c3_check"} for q in c3_exponents()]
+    return cases
+
+
+def make_ref_cases() -> None:
+    write("ref_cases.json", ref_cases())
+
+
+def _summaries(dirs: list[str]):
+    for d in dirs:
+        for js in sorted(Path(d).glob("run_*.json")):
+            r = json.loads(js.read_text())
+            if r.get("rc") == 0 and r.get("res64"):
+                yield r
+
+
+def make_ref(dirs: list[str]) -> None:
+    """Merge the reference runs summarised by oracle/run_ref.py (run_*.json:
+    Res64 of the reference's residue dump) into ref_residues.json."""
+    path = HERE / "ref_residues.json"
+    old = json.loads(path.read_text())["cases"] if path.exists() else []
+    key = lambda c: (c["q"], c["n"], c["prp"], c["iterations"])  # noqa: E731
+    merged = {key(c): c for c in old}
+    sets = {(c["q"], c["iterations"], c["prp"]): c["set"] for c in ref_cases()}
+    for r in _summaries(dirs):
+        c = {"q": r["exponent"], "n": r["n"], "prp": r["prp"], "iterations": r["iterations"],
+             "res64": r["res64"], "fft": r["fft_used"], "pool": r["pool"],
+             "per_iteration_ms": r["per_iteration_ms"], "conclusion": r["conclusion"],
+             "dump_sha256": r.get("sha256_of_dump")}
+        if (c["q"], c["iterations"], c["prp"]) in sets:
+            c["set"] = sets[(c["q"], c["iterations"], c["prp"])]
+        merged[key(c)] = c
     write("ref_residues.json", {
         "source": "reference LucasNTT build (oracle/build_ref.sh) run on a B200 by oracle/run_ref.py; "
                   "Res64 derived from its residue dump; dump_sha256 = SHA-256 of that dump file "
-                  "(LucasNTT_results.dat, 19-byte records)",
-        "cases": cases})
+                  "(19-byte records)",
+        "cases": list(merged.values())})
 
 
-def make_ref_timings() -> None:
+def make_ref_timings(dirs: list[str]) -> None:
     """Per-iteration times of the reference build at each NTT length, from the
-    oracle/run_ref.py summaries collected on a B200 (gpurun_out/ref_*/run_*.json).
-    bench.py uses them to state the reference's plain one-at-a-time tests/hour."""
-    base = ROOT / "gpurun_out"
-    by_n = {}
-    for js in sorted(base.glob("ref_*/run_*.json")):
-        r = json.loads(js.read_text())
-        if r.get("rc") != 0 or not r.get("per_iteration_ms"):
+    oracle/run_ref.py summaries (run_*.json) in the given directories, merged
+    into ref_timings.json.  bench.py uses them to state the reference's plain
+    one-at-a-time tests/hour."""
+    path = HERE / "ref_timings.json"
+    by_n = json.loads(path.read_text())["by_n"] if path.exists() else {}
+    for r in _summaries(dirs):
+        if not r.get("per_iteration_ms"):
             continue
-        by_n.setdefault(str(r["n"]), []).append({"q": r["exponent"], "prp": r["prp"], "pool": r["pool"],
-                                                 "fft": r["fft_used"], "per_iteration_us": r["per_iteration_ms"] * 1e3})
+        rows = by_n.setdefault(str(r["n"]), [])
+        row = {"q": r["exponent"], "prp": r["prp"], "pool": r["pool"], "fft": r["fft_used"],
+               "per_iteration_us": r["per_iteration_ms"] * 1e3}
+        if row not in rows:
+            rows.append(row)
     write("ref_timings.json", {
         "source": "reference LucasNTT build (oracle/build_ref.sh) run on a B200 by oracle/run_ref.py; "
                   "its own 'Per iteration (ms)' (lucas_prp.cu:319)",
@@ -140,6 +241,9 @@ def make_ref_timings() -> None:
 
 
 if __name__ == "__main__":
+    if len(sys.argv) > 1 and sys.argv[1] in ("ref", "reftimes"):
+        (make_ref if sys.argv[1] == "ref" else make_ref_timings)(sys.argv[2:])
+        raise SystemExit(0)
     sets = sys.argv[1:] or ["small"]
     for s in sets:
         if s == "small":
@@ -148,7 +252,5 @@ if __name__ == "__main__":
             make_c1()
         elif s == "c2":
             make_c2("--c2-long" in sets)
-        elif s == "ref":
-            make_ref()
-        elif s == "reftimes":
-            make_ref_timings()
+        elif s == "refcases":
+            make_ref_cases()

@@ -123,11 +123,28 @@ def test_oracle_fixtures_match_reference_build():
     c2 = json.loads((GOLDEN / "c2_oracle.json").read_text())["res64_after"]
     checked = 0
     for c in ref:
-        if (c["q"], c["n"]) in c1 and c["iterations"] == c["q"] - 2:
+        if (c["q"], c["n"]) in c1 and c["iterations"] == c["q"] - 2 and not c["prp"]:
             assert c1[(c["q"], c["n"])] == c["res64"], c
             checked += 1
-        elif c["q"] == 139000003 and str(c["iterations"]) in c2:
+        elif c["q"] == 139000003 and not c["prp"] and str(c["iterations"]) in c2:
             assert c2[str(c["iterations"])] == c["res64"], c
             checked += 1
     assert checked >= 11
-    assert {c["conclusion"] for c in ref if c["q"] == 44497} == {"Prime"}
+    assert {c["conclusion"] for c in ref if c["q"] == 44497 and not c["prp"]} == {"Prime"}
+    assert {c["conclusion"] for c in ref if c["q"] == 44497 and c["prp"]} == {"Probably Prime"}
+
+
+def test_oracle_matches_reference_build_prp_and_batch_pins(oracle_mod):
+    """The oracle's PRP mode (s0 = 3, no -2, residue 9 for primes) and a C3
+    batch exponent after 20,000 LL squarings, against the reference build's
+    residues: full PRP tests of four serving-stream exponents (n = 512, 1024)
+    and q = 100267 at n = 4096."""
+    ref = json.loads((GOLDEN / "ref_residues.json").read_text())["cases"]
+    cases = [c for c in ref if c["prp"] and c["iterations"] == c["q"] and c["q"] in (11863, 12799, 13381, 15727)]
+    cases += [c for c in ref if c["q"] == 100267 and c["iterations"] == 20000 and not c["prp"]]
+    assert len(cases) == 5
+    oracle_mod.set_threads(oracle_mod.max_threads())
+    for c in cases:
+        with oracle_mod.OracleTest(c["q"], c["n"], c["prp"]) as T:
+            T.iterate(c["iterations"])
+            assert f"{T.res64():016x}" == c["res64"], c
