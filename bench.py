@@ -53,10 +53,17 @@ def parse_args():
     ap.add_argument("--workload", choices=["c1", "c2", "c3", "c4", "c5", "lengths"], default="c2",
                     help="c2: one 8M-point LL test (default); c3/c4: batched tests/hour; c5: serving; "
                          "lengths: one LL test at each of 2^24, 2^25, 2^26")
-    ap.add_argument("--seconds", type=float, default=30.0, help="timed window of c3/c4/c5")
-    ap.add_argument("--rates", default="0.5,1,2", help="c5: arrival rates as multiples of plain capacity")
-    ap.add_argument("--c5-range", default="10000,200000",
-                    help="c5: exponent range (full tests must finish inside the timed window)")
+    ap.add_argument("--seconds", type=float, default=120.0, help="c5: arrival window")
+    ap.add_argument("--autotune-loops", type=int, default=20, help="c3/c4: autotuner squarings per candidate (0: policy plans)")
+    ap.add_argument("--plan-cache", default="", help="c3/c4: JSON plan cache file")
+    ap.add_argument("--checkpoint-every", type=int, default=20000, help="c3/c4: Res64 checkpoint interval")
+    ap.add_argument("--batch-step", type=int, default=2000, help="c3/c4/c5: squarings per engine call")
+    ap.add_argument("--c3-count", type=int, default=256, help="c3: tests of the seeded sample to run")
+    ap.add_argument("--plain", choices=["real", "per-length"], default="per-length",
+                    help="c3/c4: plain path run test by test, or summed from per-length times")
+    ap.add_argument("--rates", default="0.25,1", help="c5: arrival rates, requests per second")
+    ap.add_argument("--drain", type=float, default=60.0, help="c5: seconds the engine runs on after the window")
+    ap.add_argument("--c5-range", default="10000,30000000", help="c5: exponent range")
     return ap.parse_args()
 
 
@@ -121,14 +128,34 @@ def measured_peak_hbm():
     return 6650.0, "fallback"
 
 
+def ncu_counters() -> dict:
+    """Per-launch ncu counters of the C2 kernels (profiles/ncu_traffic.json)."""
+    p = ROOT / "profiles" / "ncu_traffic.json"
+    return json.loads(p.read_text()) if p.exists() else {}
+
+
 def ncu_traffic(kernel: str):
     """DRAM bytes per launch of `kernel` from the committed ncu summary, or None."""
-    p = ROOT / "profiles" / "ncu_traffic.json"
-    if not p.exists():
-        return None
-    d = json.loads(p.read_text())
-    v = d.get("kernels", {}).get(kernel)
+    v = ncu_counters().get("kernels", {}).get(kernel)
     return None if v is None else float(v)
+
+
+def issue_roofline(kernel: str, avg_launch_s: float, sms: int, sm_mhz):
+    """The binding roofline of the integer-bound kernels: warp instructions
+    issued per launch (ncu's count, committed) over the launch's CUDA-event
+    duration, against the SMs' issue rate (4 schedulers per SM, one warp
+    instruction per clock each) at the SM clock sampled during the timed region.
+    The ALU and FMA pipe fractions are ncu's, from the same capture."""
+    d = ncu_counters()
+    inst = d.get("warp_instructions", {}).get(kernel)
+    if inst is None or not sm_mhz:
+        return None
+    peak = sms * 4 * sm_mhz * 1e6
+    achieved = inst / avg_launch_s
+    out = {"warp_instructions_per_launch": inst, "achieved": achieved, "peak": peak,
+           "unit": "warp instructions/s", "frac": achieved / peak, "sm_mhz": sm_mhz, "sms": sms}
+    out.update({f"ncu_{k}": v for k, v in d.get("pipes", {}).get(kernel, {}).items()})
+    return out
 
 
 def cpu_port_sample(threads: int, iterations: int):
@@ -261,12 +288,80 @@ def reference_plain_tests_per_hour(cuda_b200, exps, target_of):
     return 3600 / (sum(t) / len(t))
 
 
+def c3_exponents() -> list[int]:
+    """C3: 256 primes in [1e5, 2e6], random.Random(0).sample."""
+    import random
+
+    return random.Random(0).sample(primes_between(100000, 2000000), 256)
+
+
+def c4_exponents() -> list[int]:
+    """C4: 64 primes in [5e6, 2e7], random.Random(1).sample."""
+    import random
+
+    return random.Random(1).sample(primes_between(5000000, 20000000), 64)
+
+
+def c5_pool(lo: int = 10000, hi: int = 30000000, count: int = 64) -> list[tuple[int, bool]]:
+    """C5 requests: `count` draws of (q, prp), q the smallest prime >= exp(U(ln lo,
+    ln hi)), prp by a fair coin, random.Random(2)."""
+    import bisect
+    import math
+    import random
+
+    primes = primes_between(lo, hi + 100000)
+    rng = random.Random(2)
+    out = []
+    for _ in range(count):
+        x = math.exp(rng.uniform(math.log(lo), math.log(hi)))
+        out.append((primes[min(bisect.bisect_left(primes, int(x)), len(primes) - 1)], rng.random() < 0.5))
+    return out
+
+
+def reference_pins() -> dict:
+    """(q, prp, iterations) -> Res64 of the reference build (tests/golden/ref_residues.json)."""
+    return {(c["q"], bool(c["prp"]), c["iterations"]): c["res64"] for c in reference_residues()}
+
+
+def single_test_us(cuda_b200, exponents, prp: bool, device: int, iters: int = 1000) -> dict:
+    """This repository's single-test path (one test alone, lnt_iterate), µs per
+    squaring at each policy length of `exponents`: CUDA events around `iters`
+    squarings of the first exponent of each length, after a warm-up call."""
+    import torch
+
+    out = {}
+    for q in exponents:
+        n = 1 << cuda_b200.secured_log2_length(q)
+        if n in out:
+            continue
+        stream = torch.cuda.Stream(device=device)
+        with cuda_b200.LucasTest(q, 0, prp, device=device) as t:
+            t.set_stream(stream.cuda_stream)
+            t.iterate(min(iters, 200))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            t.iterate(iters)
+            e1.record(stream)
+            e1.synchronize()
+            out[n] = e0.elapsed_time(e1) * 1e3 / iters
+    return out
+
+
 def run_batch_workload(args, exps, prp, target_of, label, config, rank=0, world=1, local_rank=0):
-    """tests/hour of the batch engine against one-test-at-a-time, on a bounded
-    window.  With N ranks (one process per GPU) each rank runs its own batch over
-    a cost-balanced share of the work list (cuda_b200/shard.py) and rank 0
-    reports the whole job: the tests all ranks advanced over the slowest rank's
-    window.  No collective touches the data path."""
+    """tests/hour of the batch engine over the whole work list, timed from the
+    first submission to the last completion (wall clock around the engine's
+    calls, which synchronise the device), with the autotuner on (plans cached
+    in --plan-cache) and Res64 checkpoints every --checkpoint-every squarings.
+    Every final Res64 and checkpoint that the reference build has a residue for
+    is compared with it; a mismatch fails the run.  With N ranks (one process
+    per GPU) each rank runs its own batch over a cost-balanced share of the
+    work list (cuda_b200/shard.py); no collective touches the data path.
+
+    The plain one-at-a-time path: --plain real runs every test alone through
+    the single-test path (lnt_iterate) back to back; --plain per-length sums
+    (squarings x µs per squaring alone at the test's length), that time
+    measured once per length.  The reference build's plain time is the same sum
+    over its own per-length time (tests/golden/ref_timings.json)."""
     import cuda_b200
     from cuda_b200 import shard
 
@@ -277,53 +372,121 @@ def run_batch_workload(args, exps, prp, target_of, label, config, rank=0, world=
         import torch
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=3600))
+    pins = reference_pins()
     mine = shard.partition_by_cost(exps, world, lambda q: shard.test_cost(q, target_of(q), prp))[rank]
-    step = 50
-    with cuda_b200.Batch(device=local_rank) as b:
-        for q in mine:
-            b.submit(q, 0, prp, target_of(q))
-        for _ in range(3):
-            b.run(step)
-        if dist is not None:
-            dist.barrier()
-        steps = 0
-        t0 = time.perf_counter()
-        while time.perf_counter() - t0 < args.seconds:
-            b.run(step)
-            steps += 1
-        elapsed = time.perf_counter() - t0
-        finished = b.poll()
-    done_local = sum(min(1.0, steps * step / target_of(q)) for q in mine)
-    done = sum(shard.gather_results([done_local], dist))
+    results, marks = {}, {}
+    if dist is not None:
+        dist.barrier()
+    t0 = time.perf_counter()
+    with cuda_b200.Batch(device=local_rank, autotune_loops=args.autotune_loops,
+                         plan_cache=args.plan_cache or None, checkpoint_every=args.checkpoint_every) as b:
+        ids = {b.submit(q, 0, prp, target_of(q)): q for q in mine}
+        t_admitted = time.perf_counter() - t0
+        while len(results) < len(ids):
+            b.run(args.batch_step)
+            for r in b.poll():
+                results[r["id"]] = r
+            for c in b.poll_checkpoints():
+                marks[(ids[c["id"]], c["iteration"])] = c
+    elapsed = time.perf_counter() - t0
+    # parity: every pinned final residue and checkpoint
+    checked, bad = 0, []
+    for i, r in results.items():
+        key = (ids[i], prp, r["iterations"])
+        if r["status"] != 0:
+            bad.append(("status", ids[i], r["status"]))
+        elif key in pins:
+            checked += 1
+            if f"{r['res64']:016x}" != pins[key]:
+                bad.append(("final", ids[i], f"{r['res64']:016x}", pins[key]))
+    for (q, it), c in marks.items():
+        key = (q, prp, it)
+        if key in pins:
+            checked += 1
+            if c["status"] != 0 or f"{c['res64']:016x}" != pins[key]:
+                bad.append(("checkpoint", q, it, f"{c['res64']:016x}", pins[key]))
+    checked = sum(shard.gather_results([checked], dist))
+    bad = shard.gather_results(bad, dist)
+    n_done = sum(shard.gather_results([len(results)], dist))
     elapsed = shard.max_over_ranks(elapsed, dist)
-    n_finished = sum(shard.gather_results([len(finished)], dist))
-    tests_per_hour = done / elapsed * 3600
-    plain_tests_per_hour = ref_plain = None
     if rank == 0:
-        # plain path: a sample spread over the exponents, each test alone on one GPU
-        sample = sorted(exps)[:: max(1, len(exps) // 12)]
-        times = [target_of(q) * plain_us_per_iteration(cuda_b200, q, prp, device=local_rank) * 1e-6
-                 for q in sample]
-        plain_tests_per_hour = 3600 / (sum(times) / len(times))
-        ref_plain = reference_plain_tests_per_hour(cuda_b200, exps, target_of)
-        line = {"metric": f"tests/hour, {label}", "value": tests_per_hour, "unit": "tests/hour",
-                "higher_is_better": True, "n_gpus": world, "data": "synthetic (seeded exponents)",
-                "dtype": "u64", "config": config,
-                "scaling": "strong" if world > 1 else "weak",
-                "plain_tests_per_hour": plain_tests_per_hour,
-                "speedup_vs_plain": tests_per_hour / plain_tests_per_hour,
-                "reference_plain_tests_per_hour": ref_plain,
-                "speedup_vs_reference_plain": tests_per_hour / ref_plain if ref_plain else None,
-                "window_s": elapsed, "squarings_per_test_in_window": steps * step,
-                "plain_sample": len(sample), "finished_in_window": n_finished}
+        lengths = {}
+        for q in exps:
+            n = 1 << cuda_b200.secured_log2_length(q)
+            lengths[n] = lengths.get(n, 0) + 1
+        alone = single_test_us(cuda_b200, sorted(exps), prp, local_rank)
+        plain_kind = args.plain
+        if plain_kind == "real":
+            pt0 = time.perf_counter()
+            for q in exps:
+                with cuda_b200.LucasTest(q, 0, prp, device=local_rank) as t:
+                    t.iterate(target_of(q))
+                    r = t.res64()
+                key = (q, prp, target_of(q))
+                if key in pins and f"{r:016x}" != pins[key]:
+                    bad.append(("plain", q, f"{r:016x}", pins[key]))
+            plain_s = time.perf_counter() - pt0
+        else:
+            plain_s = sum(target_of(q) * alone[1 << cuda_b200.secured_log2_length(q)] * 1e-6 for q in exps)
+        ref = reference_us_per_iteration()
+        try:
+            ref_plain_s = sum(target_of(q) * ref[1 << cuda_b200.secured_log2_length(q)] * 1e-6 for q in exps)
+        except KeyError:
+            ref_plain_s = None
+        tph = n_done / elapsed * 3600
+        line = {"metric": f"tests/hour, {label}", "value": tph, "unit": "tests/hour",
+                "higher_is_better": True, "n_gpus": world, "data": "seeded exponents (no synthetic data)",
+                "dtype": "u64", "config": config, "scaling": "strong" if world > 1 else "weak",
+                "tests": len(exps), "finished": n_done, "wall_s": elapsed, "admission_s": t_admitted,
+                "timing": "wall clock from the first submission to the last completion, max over ranks",
+                "autotune_loops": args.autotune_loops, "lengths": {str(k): v for k, v in sorted(lengths.items())},
+                "plain": plain_kind, "plain_s": plain_s, "plain_tests_per_hour": len(exps) / plain_s * 3600,
+                "speedup_vs_plain": tph / (len(exps) / plain_s * 3600),
+                "alone_us_per_squaring": {str(k): v for k, v in sorted(alone.items())},
+                "reference_plain_s": ref_plain_s,
+                "reference_plain_tests_per_hour": len(exps) / ref_plain_s * 3600 if ref_plain_s else None,
+                "speedup_vs_reference_plain": tph / (len(exps) / ref_plain_s * 3600) if ref_plain_s else None,
+                "parity": {"res64_checked_against_reference_build": checked, "mismatches": bad[:10],
+                           "equal_reference_build": not bad}}
         print(json.dumps(line), flush=True)
+        if bad:
+            raise SystemExit(f"bench: {len(bad)} residues differ from the reference build: {bad[:3]}")
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
 
 
 C1_EXPONENTS = [44497, 44501, 44507, 44519, 44531, 44533, 44537, 44543, 44549]
+C2_PARITY_MARKS = (1000, 10000)
+
+
+def reference_residues() -> list[dict]:
+    """The reference build's residues (tests/golden/ref_residues.json)."""
+    return json.loads((ROOT / "tests" / "golden" / "ref_residues.json").read_text())["cases"]
+
+
+def c2_parity(test) -> dict:
+    """Square the freshly initialised C2 test to 1,000 and then 10,000
+    iterations and compare its Res64 with the reference build's at those
+    marks.  A mismatch ends the run with an error: a time for a path whose
+    residues differ from the reference's is not a result."""
+    want = {c["iterations"]: c["res64"] for c in reference_residues()
+            if c["q"] == EXPONENT and c["n"] == N and not c["prp"]}
+    out, done = {}, 0
+    for mark in C2_PARITY_MARKS:
+        test.iterate(mark - done)
+        done = mark
+        got = f"{test.res64():016x}"
+        out[f"res64_{mark // 1000}k"] = got
+        if mark not in want:
+            raise SystemExit(f"bench: no reference-build Res64 for q={EXPONENT} after {mark} squarings")
+        if got != want[mark]:
+            raise SystemExit(f"bench: Res64 after {mark} squarings is {got}, the reference build's is "
+                             f"{want[mark]}: the timed path is not bit-exact")
+    out["reference_res64"] = {f"{m // 1000}k": want[m] for m in C2_PARITY_MARKS}
+    out["equal_reference_build"] = True
+    return out
 
 
 def run_c1(args):
@@ -333,8 +496,7 @@ def run_c1(args):
     committed fixture of the reference build's residues."""
     import cuda_b200
 
-    golden = json.loads((ROOT / "tests" / "golden" / "ref_residues.json").read_text())["cases"]
-    want = {c["q"]: c["res64"] for c in golden if c["n"] == 2048}
+    want = {c["q"]: c["res64"] for c in reference_residues() if c["n"] == 2048 and not c["prp"]}
     per_it, ok = [], True
     with cuda_b200.LucasTest(C1_EXPONENTS[0]) as t:  # warm-up: module load, first launch
         t.iterate(100)
@@ -379,12 +541,21 @@ def run_c1(args):
 
 
 def run_serving(args, rank=0, world=1, local_rank=0):
-    """Poisson stream of LL/PRP requests against the continuous-batching engine,
-    beside the plain sequential path (a FIFO queue over measured service times).
+    """Serving: LL/PRP requests (the seeded C5 pool: q log-uniform in
+    [1e4, 3e7], LL or PRP by a fair coin) arrive as a Poisson stream at each
+    rate of --rates (requests per second) for --seconds; the continuous-batching
+    engine admits them under a 150 GB HBM budget as they arrive and keeps every
+    residue on the device until its verdict.  After the window the engine runs
+    on for --drain seconds, then stops.  Latency = completion - arrival for the
+    requests that finished; the others are counted as unfinished with their
+    age at the stop (a lower bound on their latency) and are left out of the
+    percentiles, which the line says.  The plain path is the same arrivals
+    served one at a time in arrival order (FIFO) with service times = squarings
+    x this repository's single-test µs per squaring at the request's length
+    (measured once per length): a simulation, labelled as one.  Every finished
+    request whose full-test Res64 the reference build has is compared with it.
     With N ranks the stream's rate is N times higher and request i goes to rank
-    i mod N (round-robin dispatch to one engine per GPU); rank 0 reports the
-    percentiles over all ranks' latencies."""
-    import math
+    i mod N (round-robin dispatch to one engine per GPU)."""
     import random
 
     import numpy as np
@@ -399,77 +570,101 @@ def run_serving(args, rank=0, world=1, local_rank=0):
         import torch
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=3600))
 
     lo, hi = (int(x) for x in args.c5_range.split(","))
-    primes = primes_between(lo, min(hi * 2, hi + 100000))
+    pool = c5_pool(lo, hi)
+    pins = reference_pins()
+    alone = single_test_us(cuda_b200, sorted({q for q, _ in pool}), False, local_rank, iters=200) if rank == 0 else {}
     rng = random.Random(2)
-
-    def draw():
-        x = math.exp(rng.uniform(math.log(lo), math.log(hi)))
-        import bisect
-        return primes[min(bisect.bisect_left(primes, int(x)), len(primes) - 1)], rng.random() < 0.5
-
-    pool = [draw() for _ in range(64)]
-    service = [(q if prp else q - 2) * plain_us_per_iteration(cuda_b200, q, prp, 100, local_rank) * 1e-6
-               for q, prp in pool[:16]]
-    mean_service = sum(service) / len(service)
-    plain_capacity = 1.0 / mean_service  # tests per second, one at a time
     budget = 150 << 30
-    for mult in (float(r) for r in args.rates.split(",")):
-        rate = mult * plain_capacity * world
-        t = 0.0
-        arrivals = []
-        while t < args.seconds:
-            t += rng.expovariate(rate)
+    for rate in (float(r) for r in args.rates.split(",")):
+        t, arrivals = 0.0, []
+        while True:
+            t += rng.expovariate(rate * world)
+            if t >= args.seconds:
+                break
             q, prp = pool[rng.randrange(len(pool))]
             arrivals.append((t, q, prp))
-        arrivals = [a for a in arrivals if a[0] < args.seconds]
-        all_arrivals = arrivals
-        arrivals = arrivals[rank::world]
-        lat, done = [], 0
+        mine = arrivals[rank::world]
+        lat, unfinished, bad, checked = [], [], [], 0
+        work_done = 0.0
         if dist is not None:
             dist.barrier()
         with cuda_b200.Batch(device=local_rank, hbm_budget_bytes=budget) as b:
             t0 = time.perf_counter()
-            k, enq = 0, {}
-            while (k < len(arrivals) or done < len(arrivals)) and time.perf_counter() - t0 < 4 * args.seconds:
+            k, info = 0, {}
+            stop = args.seconds + args.drain
+            while time.perf_counter() - t0 < stop:
                 now = time.perf_counter() - t0
-                while k < len(arrivals) and arrivals[k][0] <= now:
-                    i = b.enqueue(arrivals[k][1], 0, arrivals[k][2])
-                    enq[i] = now - arrivals[k][0]  # wait before enqueue
+                while k < len(mine) and mine[k][0] <= now:
+                    i = b.enqueue(mine[k][1], 0, mine[k][2])
+                    info[i] = mine[k]
                     k += 1
-                b.run(200)
+                if k >= len(mine) and not info:
+                    break
+                if not info:  # nothing in flight: wait for the next arrival
+                    time.sleep(max(0.0, min(mine[k][0] - now, 0.05)))
+                    continue
+                b.run(args.batch_step)
+                now = time.perf_counter() - t0
                 for r in b.poll():
-                    lat.append(r["seconds"] + enq.pop(r["id"], 0.0))
-                    done += 1
+                    ta, q, prp = info.pop(r["id"])
+                    lat.append(now - ta)
+                    work_done += r["iterations"] * r["n"]
+                    key = (q, prp, q if prp else q - 2)
+                    if r["status"] != 0:
+                        bad.append(("status", q, prp, r["status"]))
+                    elif key in pins:
+                        checked += 1
+                        if f"{r['res64']:016x}" != pins[key]:
+                            bad.append((q, prp, f"{r['res64']:016x}", pins[key]))
             wall = time.perf_counter() - t0
+            unfinished = [wall - ta for ta, _, _ in info.values()]
         lat = shard.gather_results(lat, dist)
-        done = sum(shard.gather_results([done], dist))
+        unfinished = shard.gather_results(unfinished, dist)
+        bad = shard.gather_results(bad, dist)
+        checked = sum(shard.gather_results([checked], dist))
         wall = shard.max_over_ranks(wall, dist)
         if rank != 0:
             continue
-        # plain sequential path: one GPU, FIFO over the same arrivals, service =
-        # measured per-test time
-        serv = {}
-        free_at, plain_lat = 0.0, []
-        for (ta, q, prp) in all_arrivals:
-            if (q, prp) not in serv:
-                serv[(q, prp)] = (q if prp else q - 2) * plain_us_per_iteration(cuda_b200, q, prp, 100, local_rank) * 1e-6
-            start = max(free_at, ta)
-            free_at = start + serv[(q, prp)]
-            plain_lat.append(free_at - ta)
-        line = {"metric": "serving p50/p99 latency and tests/hour", "rate_multiple_of_plain_capacity": mult,
-                "requests": len(all_arrivals), "completed": done, "wall_s": wall, "n_gpus": world,
-                "p50_s": float(np.percentile(lat, 50)) if lat else None,
-                "p99_s": float(np.percentile(lat, 99)) if lat else None,
-                "tests_per_hour": done / wall * 3600,
-                "plain_p50_s": float(np.percentile(plain_lat, 50)), "plain_p99_s": float(np.percentile(plain_lat, 99)),
-                "plain_tests_per_hour": len(all_arrivals) / free_at * 3600 if free_at else None,
-                "config": {"exponents": f"primes log-uniform in [{lo}, {hi}], LL/PRP by a seeded coin (seed 2)",
-                           "hbm_budget_gb": 150, "arrival": "Poisson",
+        # plain path: FIFO over the same arrivals, one test at a time, stopped at the same time
+        free_at, plain_lat, plain_unfinished = 0.0, [], []
+        for (ta, q, prp) in arrivals:
+            n = 1 << cuda_b200.secured_log2_length(q)
+            start_t = max(free_at, ta)
+            end_t = start_t + (q if prp else q - 2) * alone[n] * 1e-6
+            if end_t <= wall:
+                plain_lat.append(end_t - ta)
+                free_at = end_t
+            else:
+                plain_unfinished.append(wall - ta)
+                free_at = max(free_at, end_t)
+        pct = lambda v, p: float(np.percentile(v, p)) if v else None  # noqa: E731
+        lens = sorted({1 << cuda_b200.secured_log2_length(q) for _, q, _ in arrivals})
+        line = {"metric": "serving p50/p99 latency and tests/hour", "rate_requests_per_s": rate * world,
+                "requests": len(arrivals), "completed": len(lat), "unfinished": len(unfinished),
+                "wall_s": wall, "n_gpus": world,
+                "p50_s": pct(lat, 50), "p99_s": pct(lat, 99), "tests_per_hour": len(lat) / wall * 3600,
+                "unfinished_age_s": {"min": min(unfinished) if unfinished else None,
+                                     "max": max(unfinished) if unfinished else None},
+                "percentiles": "over completed requests; unfinished requests are excluded (their latency "
+                               "is at least their age at the stop)",
+                "plain": "simulated FIFO, one test at a time, service = squarings x measured single-test "
+                         "µs per squaring at the request's length",
+                "plain_completed": len(plain_lat), "plain_unfinished": len(plain_unfinished),
+                "plain_p50_s": pct(plain_lat, 50), "plain_p99_s": pct(plain_lat, 99),
+                "plain_tests_per_hour": len(plain_lat) / wall * 3600,
+                "lengths_requested": lens,
+                "parity": {"res64_checked_against_reference_build": checked, "mismatches": bad[:10],
+                           "equal_reference_build": not bad},
+                "config": {"exponents": f"seeded pool of 64: q log-uniform in [{lo}, {hi}], LL/PRP by a "
+                                        "fair coin (random.Random(2))", "window_s": args.seconds,
+                           "drain_s": args.drain, "hbm_budget_gb": 150, "arrival": "Poisson",
                            "dispatch": "round-robin over ranks" if world > 1 else "one engine"}}
         print(json.dumps(line), flush=True)
+        if bad:
+            raise SystemExit(f"bench: serving residues differ from the reference build: {bad[:3]}")
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -493,14 +688,17 @@ def main():
         import random
 
         if args.workload == "c3":
-            exps = random.Random(0).sample(primes_between(100000, 2000000), 256)
-            run_batch_workload(args, exps, False, lambda q: q - 2, "256 full LL tests, q in [1e5, 2e6] (seed 0)",
-                               {"workload": "C3 batch", "count": 256, "lengths": "4K-128K"},
+            exps = c3_exponents()[:args.c3_count]
+            run_batch_workload(args, exps, False, lambda q: q - 2,
+                               f"{len(exps)} full LL tests, q in [1e5, 2e6] (seed 0)",
+                               {"workload": "C3 batch", "count": len(exps), "lengths": "4K-128K",
+                                "subset": "the first tests of the seeded sample" if len(exps) < 256 else "all"},
                                rank, world, local_rank)
         elif args.workload == "c4":
-            exps = random.Random(1).sample(primes_between(5000000, 20000000), 64)
-            run_batch_workload(args, exps, True, lambda q: 20000, "64 PRP tests x 20000 squarings, q in [5e6, 2e7] (seed 1)",
-                               {"workload": "C4 batch", "count": 64, "lengths": "512K-1M"},
+            exps = c4_exponents()
+            run_batch_workload(args, exps, True, lambda q: 20000,
+                               "64 PRP tests x 20000 squarings, q in [5e6, 2e7] (seed 1)",
+                               {"workload": "C4 batch", "count": 64, "lengths": "256K-1M"},
                                rank, world, local_rank)
         else:
             run_serving(args, rank, world, local_rank)
@@ -530,7 +728,11 @@ def main():
         with torch.cuda.stream(stream):
             flush.random_(0, 255)
 
-    # warm-up steps (untimed)
+    # parity of the timed path before timing: Res64 after 1,000 and 10,000
+    # squarings against the reference build's residues of this exact test
+    parity = c2_parity(test)
+
+    # warm-up steps (untimed), continuing the same test
     for _ in range(args.warmup):
         flush_l2()
         test.iterate(ips)
@@ -609,6 +811,8 @@ def main():
     achieved = algo_bytes / avg_s / 1e9
     peak, peak_kind = measured_peak_hbm()
     traffic = ncu_traffic(dom_name)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    issue = issue_roofline(dom_name, avg_s, sms, (clk or {}).get("sm_mhz"))
     # every timed step launches the same kernels as the profiled one
     launches_in_timed = sum(a[0] for a in kernels.values()) * (args.steps + 1)
 
@@ -634,11 +838,12 @@ def main():
                        "reference_build_us_per_iteration": reference_us_per_iteration().get(N)},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": N * 8, "d2h_bytes_per_step": N * 8,
                     "wall_s": wall},
+            "parity": parity,
             "gpu_launches": launches_in_timed,
             "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "algo_bytes_per_launch": algo_bytes,
-                         "avg_launch_us": avg_s * 1e6},
+                         "avg_launch_us": avg_s * 1e6, "issue": issue},
             "kernels": {k: {"launches": v[0], "avg_us": v[1] * 1e3 / v[0]} for k, v in kernels.items()},
             "clocks": clk,
             "cpu_baseline": cpu,

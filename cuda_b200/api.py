@@ -43,12 +43,19 @@ class BatchResult(ctypes.Structure):
                 ("prp", ctypes.c_int), ("is_prime", ctypes.c_int), ("status", ctypes.c_int)]
 
 
-class PlanOptions(ctypes.Structure):
-    """lnt_plan_options: kernel family (1 resident, 2 radix-16, 3 radix-2), log2 n2, tile."""
-    _fields_ = [("kind", ctypes.c_uint32), ("log2_rows", ctypes.c_uint32), ("tile", ctypes.c_uint32)]
+class BatchCheckpoint(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_uint64), ("iteration", ctypes.c_uint64), ("res64", ctypes.c_uint64),
+                ("status", ctypes.c_int)]
 
-    def as_tuple(self) -> tuple[int, int, int]:
-        return int(self.kind), int(self.log2_rows), int(self.tile)
+
+class PlanOptions(ctypes.Structure):
+    """lnt_plan_options: kernel family (1 resident, 2 register passes, 3 radix-2),
+    log2 n2, tile, largest pass radix (8/16), fused (1) or two launches (2)."""
+    _fields_ = [("kind", ctypes.c_uint32), ("log2_rows", ctypes.c_uint32), ("tile", ctypes.c_uint32),
+                ("radix", ctypes.c_uint32), ("fused", ctypes.c_uint32)]
+
+    def as_tuple(self) -> tuple[int, int, int, int, int]:
+        return int(self.kind), int(self.log2_rows), int(self.tile), int(self.radix), int(self.fused)
 
 
 class LucasNTTError(RuntimeError):
@@ -113,6 +120,9 @@ def lib() -> ctypes.CDLL:
         "lnt_debug_corrupt": ([vp, u32], i32),
         "lnt_debug_corrupt_add": ([vp, u32, ctypes.c_int64], i32),
         "lnt_batch_use_graphs": ([vp, i32], i32),
+        "lnt_batch_checkpoint_every": ([vp, u64], i32),
+        "lnt_batch_poll_checkpoints": ([vp, ctypes.POINTER(BatchCheckpoint), i32, ctypes.POINTER(i32)], i32),
+        "lnt_batch_plan_cache": ([vp, cp], i32),
         "lnt_arith_selftest": ([i32, ctypes.POINTER(u64), ctypes.POINTER(u64)], i32),
     }
     for name, (args, res) in sigs.items():
@@ -155,15 +165,15 @@ def check_provided_length(exponent: int, description: str) -> int:
     return int(d.value)
 
 
-def plan_candidates(exponent: int, n: int = 0) -> list[tuple[int, int, int]]:
-    """Every valid plan (kind, log2 n2, tile) for (q, n): lnt_plan_candidates."""
-    buf = (PlanOptions * 64)()
+def plan_candidates(exponent: int, n: int = 0) -> list[tuple[int, int, int, int, int]]:
+    """Every valid plan (kind, log2 n2, tile, radix, fused) for (q, n): lnt_plan_candidates."""
+    buf = (PlanOptions * 128)()
     c = ctypes.c_int()
-    _check(lib().lnt_plan_candidates(exponent, n, buf, 64, ctypes.byref(c)), "lnt_plan_candidates")
-    return [buf[i].as_tuple() for i in range(min(c.value, 64))]
+    _check(lib().lnt_plan_candidates(exponent, n, buf, 128, ctypes.byref(c)), "lnt_plan_candidates")
+    return [buf[i].as_tuple() for i in range(min(c.value, 128))]
 
 
-def plan_describe(plan: tuple[int, int, int], exponent: int, n: int = 0) -> str:
+def plan_describe(plan: tuple[int, ...], exponent: int, n: int = 0) -> str:
     buf = ctypes.create_string_buffer(128)
     o = PlanOptions(*plan)
     _check(lib().lnt_plan_describe(ctypes.byref(o), exponent, n, buf, 128), "lnt_plan_describe")
@@ -181,19 +191,19 @@ def arith_selftest(device: int = 0) -> int:
 
 def autotune(exponent: int, n: int = 0, prp: bool = False, device: int = 0, loops: int = 100):
     """lnt_autotune: [(plan, ms for `loops` squarings or -1)], index of the fastest."""
-    tried = (PlanOptions * 64)()
-    ms = (ctypes.c_float * 64)()
+    tried = (PlanOptions * 128)()
+    ms = (ctypes.c_float * 128)()
     c, b = ctypes.c_int(), ctypes.c_int()
-    _check(lib().lnt_autotune(exponent, n, int(bool(prp)), device, loops, tried, ms, 64, ctypes.byref(c),
+    _check(lib().lnt_autotune(exponent, n, int(bool(prp)), device, loops, tried, ms, 128, ctypes.byref(c),
                               ctypes.byref(b)), "lnt_autotune")
-    return [(tried[i].as_tuple(), float(ms[i])) for i in range(min(c.value, 64))], int(b.value)
+    return [(tried[i].as_tuple(), float(ms[i])) for i in range(min(c.value, 128))], int(b.value)
 
 
 class LucasTest:
     """One Lucas-Lehmer (prp=False) or base-3 PRP test of M = 2^exponent - 1."""
 
     def __init__(self, exponent: int, n: int = 0, prp: bool = False, device: int = 0,
-                 plan: tuple[int, int, int] | None = None):
+                 plan: tuple[int, ...] | None = None):
         h = ctypes.c_void_p()
         if plan is None:
             _check(lib().lnt_create(exponent, n, int(bool(prp)), device, ctypes.byref(h)), "lnt_create")
@@ -268,7 +278,7 @@ class LucasTest:
         _check(lib().lnt_plan_name(self._h, buf, 64), "lnt_plan_name")
         return buf.value.decode()
 
-    def plan_options(self) -> tuple[int, int, int]:
+    def plan_options(self) -> tuple[int, int, int, int, int]:
         o = PlanOptions()
         _check(lib().lnt_get_plan(self._h, ctypes.byref(o)), "lnt_get_plan")
         return o.as_tuple()
@@ -315,12 +325,16 @@ class Batch:
     as they finish (lnt_batch_*)."""
 
     def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, autotune_loops: int = 0,
-                 graphs: bool = True):
+                 graphs: bool = True, checkpoint_every: int = 0, plan_cache: str | None = None):
         h = ctypes.c_void_p()
         _check(lib().lnt_batch_create(device, int(hbm_budget_bytes), ctypes.byref(h)), "lnt_batch_create")
         self._h = h
+        if plan_cache:
+            _check(lib().lnt_batch_plan_cache(self._h, str(plan_cache).encode()), "lnt_batch_plan_cache")
         if autotune_loops:
             _check(lib().lnt_batch_autotune(self._h, int(autotune_loops)), "lnt_batch_autotune")
+        if checkpoint_every:
+            _check(lib().lnt_batch_checkpoint_every(self._h, int(checkpoint_every)), "lnt_batch_checkpoint_every")
         if not graphs:
             _check(lib().lnt_batch_use_graphs(self._h, 0), "lnt_batch_use_graphs")
 
@@ -377,6 +391,18 @@ class Batch:
                             "iterations": r.iterations, "res64": r.res64, "is_prime": bool(r.is_prime),
                             "status": r.status, "seconds": r.seconds})
             if c.value < 64:
+                return out
+
+    def poll_checkpoints(self) -> list[dict]:
+        """Res64 checkpoints recorded since the last call: {id, iteration, res64, status}."""
+        out = []
+        buf = (BatchCheckpoint * 256)()
+        while True:
+            c = ctypes.c_int()
+            _check(lib().lnt_batch_poll_checkpoints(self._h, buf, 256, ctypes.byref(c)), "lnt_batch_poll_checkpoints")
+            out += [{"id": buf[k].id, "iteration": buf[k].iteration, "res64": buf[k].res64,
+                     "status": buf[k].status} for k in range(c.value)]
+            if c.value < 256:
                 return out
 
     def status(self) -> tuple[int, int]:

@@ -20,6 +20,10 @@
 
 namespace lnt {
 struct Gerbicz;
+struct Jacobi;
+bool jacobi_available(std::string* why);
+int jacobi_of_ll_residue(const uint64_t* digits, const uint8_t* widths, uint32_t n, uint32_t q,
+                         std::string* why);
 }
 
 struct lnt_test {
@@ -66,6 +70,7 @@ struct lnt_test {
   cudaGraphExec_t graph = nullptr;
   bool graph_failed = false;    // capture unavailable on this stream: plain launches
   lnt::Gerbicz* gz = nullptr;   // PRP error check (lnt_gerbicz_enable), or none
+  lnt::Jacobi* jc = nullptr;    // LL error check (lnt_jacobi_enable), or none
 };
 
 namespace {
@@ -106,9 +111,11 @@ cudaError_t dalloc(T** p, size_t count) {
 }
 
 void free_gerbicz(lnt_test* t);
+void free_jacobi(lnt_test* t);
 
 void free_all(lnt_test* t) {
   free_gerbicz(t);
+  free_jacobi(t);
   void* ptrs[] = {t->x, t->w, t->uw, t->widths, t->status, t->rt, t->irt, t->rdesc, t->tdesc,
                   t->twf, t->twi, t->rt1, t->irt1, t->rt2, t->irt2, t->itw1, t->iitw1,
                   t->itw2, t->iitw2, t->wt, t->uwt, t->widt, t->carry, t->fuse, t->canon,
@@ -142,12 +149,12 @@ void power_table(uint32_t n, bool inverse, std::vector<uint64_t>& out) {
 // Inter-pass twiddles of a length-n radix-16 transform in pass order: pass j
 // (span s, radix R, q = s / R) holds, for each task t < q, the run
 // omega_n^(t brev_R(r) n / s), r < R.  The last pass (q = 1) has none.
-void pass_table(uint32_t n, bool inverse, std::vector<uint64_t>& out) {
+void pass_table(uint32_t n, uint32_t max_radix, bool inverse, std::vector<uint64_t>& out) {
   uint32_t log2n = 0;
   while ((1u << log2n) < n) ++log2n;
   std::vector<uint64_t> pw;
   power_table(n, inverse, pw);
-  const std::vector<uint32_t> radix = lnt::r16_pass_radices(log2n);
+  const std::vector<uint32_t> radix = lnt::r16_pass_radices(log2n, max_radix);
   out.clear();
   uint32_t span = n;
   for (size_t j = 0; j + 1 < radix.size(); ++j) {
@@ -165,12 +172,13 @@ void pass_table(uint32_t n, bool inverse, std::vector<uint64_t>& out) {
   if (out.empty()) out.push_back(1);  // keep the pointer valid
 }
 
-// full = false: root_table (n/2 entries); full = true: pass_table
-int upload_roots(lnt_test* t, uint32_t n, uint64_t** rt, uint64_t** irt, bool full = false) {
+// max_radix = 0: root_table (n/2 entries); 8 or 16: pass_table of passes of
+// at most that radix
+int upload_roots(lnt_test* t, uint32_t n, uint64_t** rt, uint64_t** irt, uint32_t max_radix = 0) {
   std::vector<uint64_t> a, b;
-  if (full) {
-    pass_table(n, false, a);
-    pass_table(n, true, b);
+  if (max_radix) {
+    pass_table(n, max_radix, false, a);
+    pass_table(n, max_radix, true, b);
   } else {
     root_table(n, false, a);
     root_table(n, true, b);
@@ -215,6 +223,7 @@ lnt::TwoPassDesc twopass_desc(const lnt_test* t) {
   d.tile = t->plan.tile;
   d.ntiles = t->plan.ntiles;
   d.prp = (uint32_t)t->prp;
+  d.radix = t->plan.radix;
   return d;
 }
 
@@ -776,6 +785,121 @@ int gerbicz_iterate(lnt_test* t, uint64_t iterations) {
   return LNT_OK;
 }
 
+// ---- Jacobi check for LL tests (lnt_jacobi.cpp has the symbol) ----------
+//
+// Every `interval` squarings the residue's symbol (s - 2 | M_q) must be -1; a
+// residue that passes becomes the verified one, a residue that fails (or a
+// carry flag raised by the kernels) sends the test back to the last verified
+// residue, and the squarings since are redone.
+
+}  // namespace
+
+namespace lnt {
+struct Jacobi {
+  uint64_t interval = 0;
+  StateBuf ok;  // the last residue whose symbol was -1 (or the state when the check began)
+  uint64_t done = 0, verified = 0, checks = 0, errors = 0;
+  uint32_t failed_in_a_row = 0;
+};
+}  // namespace lnt
+
+namespace {
+
+void free_jacobi(lnt_test* t) {
+  if (!t->jc) return;
+  free_state(t->jc->ok);
+  delete t->jc;
+  t->jc = nullptr;
+}
+
+int save_state_buf(lnt_test* t, lnt::StateBuf& dst) {
+  LNT_CUDA(cudaMemcpyAsync(dst.x, t->x, (size_t)t->n * 8, cudaMemcpyDeviceToDevice, t->stream), "copy state");
+  if (carry_words(t))
+    LNT_CUDA(cudaMemcpyAsync(dst.carry, t->carry, carry_words(t) * 8, cudaMemcpyDeviceToDevice, t->stream),
+             "copy carries");
+  dst.canonical_input = t->canonical_input;
+  dst.pending_carries = t->pending_carries;
+  dst.pristine = t->pristine;
+  dst.zero_start = t->zero_start;
+  return LNT_OK;
+}
+
+int load_state_buf(lnt_test* t, const lnt::StateBuf& src) {
+  LNT_CUDA(cudaMemcpyAsync(t->x, src.x, (size_t)t->n * 8, cudaMemcpyDeviceToDevice, t->stream), "copy state");
+  if (carry_words(t))
+    LNT_CUDA(cudaMemcpyAsync(t->carry, src.carry, carry_words(t) * 8, cudaMemcpyDeviceToDevice, t->stream),
+             "copy carries");
+  t->canonical_input = src.canonical_input;
+  t->pending_carries = src.pending_carries;
+  t->pristine = src.pristine;
+  t->zero_start = src.zero_start;
+  t->canon_valid = false;
+  return LNT_OK;
+}
+
+int jacobi_rebase(lnt_test* t) {
+  lnt::Jacobi& j = *t->jc;
+  const int st = save_state_buf(t, j.ok);
+  LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
+  j.done = j.verified = 0;
+  j.failed_in_a_row = 0;
+  return st;
+}
+
+// The symbol (s - 2 | M_q) of the current residue; a raised carry flag counts
+// as a failed check (symbol 0).
+int jacobi_symbol(lnt_test* t, int& symbol) {
+  uint32_t flags = 0;
+  int st = read_status(t, flags);
+  if (st != LNT_OK) return st;
+  if (flags & lnt::kStatusCarryOverflow) {
+    symbol = 0;
+    return LNT_OK;
+  }
+  if ((st = canonicalize(t)) != LNT_OK) return st;
+  std::vector<uint64_t> d(t->n);
+  LNT_CUDA(cudaMemcpyAsync(d.data(), t->canon, (size_t)t->n * 8, cudaMemcpyDeviceToHost, t->stream),
+           "download digits");
+  LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
+  std::string why;
+  symbol = lnt::jacobi_of_ll_residue(d.data(), t->h_widths.data(), t->n, t->q, &why);
+  if (symbol == 2) return fail(LNT_ERR_UNSUPPORTED_LENGTH, "Jacobi check: " + why);
+  return LNT_OK;
+}
+
+int jacobi_iterate(lnt_test* t, uint64_t iterations) {
+  lnt::Jacobi& j = *t->jc;
+  uint64_t left = iterations;
+  while (left) {
+    const uint64_t step = std::min<uint64_t>(left, j.interval - j.done % j.interval);
+    int st = queue_iterations(t, step, nullptr);
+    if (st != LNT_OK) return st;
+    j.done += step;
+    left -= step;
+    if (j.done % j.interval != 0) continue;
+    int symbol = 0;
+    if ((st = jacobi_symbol(t, symbol)) != LNT_OK) return st;
+    if (symbol == -1) {
+      if ((st = save_state_buf(t, j.ok)) != LNT_OK) return st;
+      LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
+      j.verified = j.done;
+      j.failed_in_a_row = 0;
+      ++j.checks;
+      continue;
+    }
+    ++j.errors;
+    if (++j.failed_in_a_row > kGerbiczRetries)
+      return fail(LNT_ERR_NUMERIC, "Jacobi check: the same squarings failed " +
+                                       std::to_string(kGerbiczRetries) + " times in a row");
+    if ((st = load_state_buf(t, j.ok)) != LNT_OK) return st;
+    LNT_CUDA(cudaMemsetAsync(t->status, 0, 4, t->stream), "clear status");
+    LNT_CUDA(cudaStreamSynchronize(t->stream), "synchronize");
+    left += j.done - j.verified;
+    j.done = j.verified;
+  }
+  return LNT_OK;
+}
+
 }  // namespace
 
 namespace lnt {
@@ -834,6 +958,22 @@ uint64_t test_device_bytes(uint32_t n) {
 }
 }  // namespace lnt
 
+namespace {
+lnt::PlanOptions from_abi(const lnt_plan_options& o) {
+  lnt::PlanOptions p;
+  p.kind = o.kind;
+  p.log2_rows = o.log2_rows;
+  p.tile = o.tile;
+  p.radix = o.radix;
+  p.fused = o.fused;
+  return p;
+}
+
+lnt_plan_options to_abi(const lnt::PlanOptions& p) {
+  return {p.kind, p.log2_rows, p.tile, p.radix, p.fused};
+}
+}  // namespace
+
 extern "C" {
 
 const char* lnt_status_string(int status) {
@@ -868,11 +1008,7 @@ int lnt_create_with_plan(uint32_t exponent, uint32_t n, int prp, int device,
   }
   lnt::Plan plan;
   lnt::PlanOptions opt;
-  if (options) {
-    opt.kind = options->kind;
-    opt.log2_rows = options->log2_rows;
-    opt.tile = options->tile;
-  }
+  if (options) opt = from_abi(*options);
   std::string why;
   if (!lnt::make_plan(n, exponent, &opt, plan, &why)) return fail(LNT_ERR_UNSUPPORTED_LENGTH, why);
   if (n > exponent) return fail(LNT_ERR_UNSUPPORTED_LENGTH, "length exceeds the exponent");
@@ -919,14 +1055,14 @@ int lnt_create_with_plan(uint32_t exponent, uint32_t n, int prp, int device,
 
   int st;
   if (plan.kind == lnt::PlanKind::Resident) {
-    if ((st = upload_roots(t, n, &t->rt, &t->irt, true)) != LNT_OK) return bail(st);
+    if ((st = upload_roots(t, n, &t->rt, &t->irt, 8)) != LNT_OK) return bail(st);  // the resident kernel's passes
     if ((e = dalloc(&t->rdesc, 1))) return bail(cuda_fail(e, "allocate descriptor"));
   } else {
     if ((st = upload_roots(t, plan.n1, &t->rt1, &t->irt1)) != LNT_OK) return bail(st);
     if ((st = upload_roots(t, plan.n2, &t->rt2, &t->irt2)) != LNT_OK) return bail(st);
     if (plan.fast) {
-      if ((st = upload_roots(t, plan.n1, &t->itw1, &t->iitw1, true)) != LNT_OK) return bail(st);
-      if ((st = upload_roots(t, plan.n2, &t->itw2, &t->iitw2, true)) != LNT_OK) return bail(st);
+      if ((st = upload_roots(t, plan.n1, &t->itw1, &t->iitw1, plan.radix)) != LNT_OK) return bail(st);
+      if ((st = upload_roots(t, plan.n2, &t->itw2, &t->iitw2, plan.radix)) != LNT_OK) return bail(st);
       if ((e = dalloc(&t->wt, n)) || (e = dalloc(&t->uwt, n)) || (e = dalloc(&t->widt, n)) ||
           (e = lnt::launch_tile_major(t->w, t->uw, t->widths, plan.n1, plan.n2, plan.tile, t->wt,
                                       t->uwt, t->widt, t->stream)))
@@ -974,6 +1110,7 @@ int lnt_init_test(lnt_test* t) {
   d[0] = t->prp ? 3 : 4;
   int st = upload_digits(t, d.data());
   if (st == LNT_OK && t->gz) st = gerbicz_rebase(t);
+  if (st == LNT_OK && t->jc) st = jacobi_rebase(t);
   return st;
 }
 
@@ -982,6 +1119,7 @@ int lnt_set_digits(lnt_test* t, const uint64_t* digits, size_t n) {
   DeviceGuard guard(t->device);
   int st = upload_digits(t, digits);
   if (st == LNT_OK && t->gz) st = gerbicz_rebase(t);
+  if (st == LNT_OK && t->jc) st = jacobi_rebase(t);
   return st;
 }
 
@@ -990,7 +1128,58 @@ int lnt_iterate(lnt_test* t, uint64_t iterations) {
   if (iterations == 0) return LNT_OK;
   DeviceGuard guard(t->device);
   if (t->gz) return gerbicz_iterate(t, iterations);
+  if (t->jc) return jacobi_iterate(t, iterations);
   return queue_iterations(t, iterations, nullptr);
+}
+
+int lnt_jacobi_of_digits(const uint64_t* digits, const uint8_t* widths, uint32_t n, uint32_t exponent,
+                         int* symbol) {
+  if (!digits || !widths || !symbol || n == 0 || exponent < 3)
+    return fail(LNT_ERR_INVALID_ARGUMENT, "null argument or bad size");
+  std::string why;
+  const int r = lnt::jacobi_of_ll_residue(digits, widths, n, exponent, &why);
+  if (r == 2) return fail(LNT_ERR_UNSUPPORTED_LENGTH, "Jacobi symbol: " + why);
+  *symbol = r;
+  return LNT_OK;
+}
+
+int lnt_jacobi_check(lnt_test* t, int* symbol) {
+  if (!t || !symbol) return fail(LNT_ERR_INVALID_ARGUMENT, "null argument");
+  if (t->prp) return fail(LNT_ERR_INVALID_ARGUMENT, "the Jacobi check applies to LL tests");
+  DeviceGuard guard(t->device);
+  return jacobi_symbol(t, *symbol);
+}
+
+int lnt_jacobi_enable(lnt_test* t, uint64_t interval) {
+  if (!t) return fail(LNT_ERR_INVALID_ARGUMENT, "null test");
+  DeviceGuard guard(t->device);
+  if (interval == 0) {
+    free_jacobi(t);
+    return LNT_OK;
+  }
+  if (t->prp) return fail(LNT_ERR_INVALID_ARGUMENT, "the Jacobi check applies to LL tests");
+  std::string why;
+  if (!lnt::jacobi_available(&why)) return fail(LNT_ERR_UNSUPPORTED_LENGTH, "Jacobi check: " + why);
+  free_jacobi(t);
+  t->jc = new lnt::Jacobi();
+  t->jc->interval = interval;
+  cudaError_t e = dalloc(&t->jc->ok.x, t->n);
+  if (e == cudaSuccess && carry_words(t)) e = dalloc(&t->jc->ok.carry, carry_words(t));
+  if (e != cudaSuccess) {
+    free_jacobi(t);
+    return cuda_fail(e, "allocate the Jacobi check's state");
+  }
+  const int st = jacobi_rebase(t);
+  if (st != LNT_OK) free_jacobi(t);
+  return st;
+}
+
+int lnt_jacobi_stats(lnt_test* t, uint64_t* verified_iterations, uint64_t* checks, uint64_t* errors) {
+  if (!t || !t->jc) return fail(LNT_ERR_INVALID_ARGUMENT, "no Jacobi check on this test");
+  if (verified_iterations) *verified_iterations = t->jc->verified;
+  if (checks) *checks = t->jc->checks;
+  if (errors) *errors = t->jc->errors;
+  return LNT_OK;
 }
 
 int lnt_gerbicz_enable(lnt_test* t, uint32_t block) {
@@ -1141,6 +1330,8 @@ int lnt_get_plan(lnt_test* t, lnt_plan_options* out) {
                                                 : (p.fast ? LNT_PLAN_RADIX16 : LNT_PLAN_RADIX2);
   out->log2_rows = p.kind == lnt::PlanKind::Resident ? 0 : p.log2n2;
   out->tile = p.kind == lnt::PlanKind::Resident ? 0 : p.tile;
+  out->radix = p.fast ? p.radix : 0;
+  out->fused = p.fast ? (p.fused ? 1 : 2) : 0;
   return LNT_OK;
 }
 
@@ -1149,7 +1340,7 @@ int lnt_plan_candidates(uint32_t exponent, uint32_t n, lnt_plan_options* out, in
   if (n == 0) n = 1u << lnt_secured_log2_length(exponent);
   const std::vector<lnt::PlanOptions> c = lnt::plan_candidates(n, exponent);
   *count = (int)c.size();
-  for (int i = 0; i < cap && i < (int)c.size(); ++i) out[i] = {c[i].kind, c[i].log2_rows, c[i].tile};
+  for (int i = 0; i < cap && i < (int)c.size(); ++i) out[i] = to_abi(c[i]);
   return c.empty() ? fail(LNT_ERR_UNSUPPORTED_LENGTH, "no plan for this length") : LNT_OK;
 }
 
@@ -1158,10 +1349,7 @@ int lnt_plan_describe(const lnt_plan_options* o, uint32_t exponent, uint32_t n, 
   if (!o || !out || outlen == 0) return fail(LNT_ERR_INVALID_ARGUMENT, "null argument");
   if (n == 0) n = 1u << lnt_secured_log2_length(exponent);
   lnt::Plan plan;
-  lnt::PlanOptions opt;
-  opt.kind = o->kind;
-  opt.log2_rows = o->log2_rows;
-  opt.tile = o->tile;
+  const lnt::PlanOptions opt = from_abi(*o);
   std::string why;
   if (!lnt::make_plan(n, exponent, &opt, plan, &why)) return fail(LNT_ERR_UNSUPPORTED_LENGTH, why);
   std::snprintf(out, outlen, "%s", plan.name.c_str());
@@ -1215,7 +1403,7 @@ int lnt_autotune(uint32_t exponent, uint32_t n, int prp, int device, uint32_t lo
   if (n == 0) n = 1u << lnt_secured_log2_length(exponent);
   const std::vector<lnt::PlanOptions> c = lnt::plan_candidates(n, exponent);
   std::vector<lnt_plan_options> plans;
-  for (const auto& o : c) plans.push_back({o.kind, o.log2_rows, o.tile});
+  for (const auto& o : c) plans.push_back(to_abi(o));
   std::vector<float> t(plans.size(), -1.0f);
   *count = (int)plans.size();
   *best = -1;

@@ -21,8 +21,14 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
 #include <deque>
+#include <fstream>
 #include <map>
+#include <sstream>
+#include <string>
 #include <vector>
 
 #include "../../include/lucasntt.h"
@@ -40,6 +46,7 @@ struct Entry {
   uint64_t target, done;
   uint64_t bytes;
   Clock::time_point submitted;
+  uint64_t last_checkpoint = 0;  // squaring count of the last recorded checkpoint
 };
 
 struct Pending {
@@ -104,6 +111,11 @@ struct lnt_batch {
   // autotuned plans: (n, shortest valid run) -> plan; loops = 0: policy plans
   uint32_t tune_loops = 0;
   std::map<uint64_t, lnt_plan_options> tuned;
+  std::map<uint64_t, float> tuned_ms;  // time of `tune_loops` squarings of the chosen plan
+  std::string cache_path;              // JSON plan cache ("" = none)
+  // Res64 checkpoints every `checkpoint_every` squarings (0 = none)
+  uint64_t checkpoint_every = 0;
+  std::deque<lnt_batch_checkpoint> checkpoints;
 };
 
 namespace {
@@ -326,6 +338,85 @@ int lnt_batch_destroy(lnt_batch* b) {
 
 namespace {
 
+// ---- JSON plan cache: {"device": NAME, "plans": [{"n": .., "run": .., "kind": ..,
+// "log2_rows": .., "tile": .., "radix": .., "fused": .., "ms": .., "loops": ..}, ...]}
+
+std::string device_name(int device) {
+  cudaDeviceProp prop{};
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return "unknown";
+  return prop.name;
+}
+
+void save_plan_cache(const lnt_batch* b) {
+  std::ostringstream o;
+  o << "{\n \"device\": \"" << device_name(b->device) << "\",\n \"plans\": [";
+  bool first = true;
+  for (const auto& kv : b->tuned) {
+    const lnt_plan_options& p = kv.second;
+    if (p.kind == 0) continue;  // tuning failed: nothing to keep
+    auto ms = b->tuned_ms.find(kv.first);
+    o << (first ? "\n" : ",\n") << "  {\"n\": " << (kv.first >> 8) << ", \"run\": " << (kv.first & 0xFF)
+      << ", \"kind\": " << p.kind << ", \"log2_rows\": " << p.log2_rows << ", \"tile\": " << p.tile
+      << ", \"radix\": " << p.radix << ", \"fused\": " << p.fused
+      << ", \"ms\": " << (ms == b->tuned_ms.end() ? -1.0f : ms->second) << ", \"loops\": " << b->tune_loops
+      << "}";
+    first = false;
+  }
+  o << "\n ]\n}\n";
+  const std::string tmp = b->cache_path + ".tmp";
+  {
+    std::ofstream f(tmp, std::ios::trunc);
+    if (!f) return;
+    f << o.str();
+  }
+  std::rename(tmp.c_str(), b->cache_path.c_str());
+}
+
+// The number after "key": inside one plan object (text between braces).
+bool json_number(const std::string& obj, const char* key, double& out) {
+  const std::string k = std::string("\"") + key + "\"";
+  size_t pos = obj.find(k);
+  if (pos == std::string::npos) return false;
+  pos = obj.find(':', pos + k.size());
+  if (pos == std::string::npos) return false;
+  char* end = nullptr;
+  out = std::strtod(obj.c_str() + pos + 1, &end);
+  return end != obj.c_str() + pos + 1;
+}
+
+// Loads the plans measured on a device of this batch's device name.
+void load_plan_cache(lnt_batch* b) {
+  std::ifstream f(b->cache_path);
+  if (!f) return;
+  std::stringstream ss;
+  ss << f.rdbuf();
+  const std::string text = ss.str();
+  const size_t dk = text.find("\"device\"");
+  if (dk == std::string::npos) return;
+  const size_t q0 = text.find('"', text.find(':', dk) + 1);
+  const size_t q1 = q0 == std::string::npos ? q0 : text.find('"', q0 + 1);
+  if (q1 == std::string::npos || text.substr(q0 + 1, q1 - q0 - 1) != device_name(b->device)) return;
+  size_t pos = text.find("\"plans\"");
+  while (pos != std::string::npos) {
+    const size_t o0 = text.find('{', pos);
+    if (o0 == std::string::npos) break;
+    const size_t o1 = text.find('}', o0);
+    if (o1 == std::string::npos) break;
+    const std::string obj = text.substr(o0, o1 - o0 + 1);
+    double n, run, kind, rows, tile, radix, fused, ms = -1;
+    if (json_number(obj, "n", n) && json_number(obj, "run", run) && json_number(obj, "kind", kind) &&
+        json_number(obj, "log2_rows", rows) && json_number(obj, "tile", tile) &&
+        json_number(obj, "radix", radix) && json_number(obj, "fused", fused)) {
+      json_number(obj, "ms", ms);
+      const uint64_t key = ((uint64_t)n << 8) | ((uint64_t)run & 0xFF);
+      lnt_plan_options p{(uint32_t)kind, (uint32_t)rows, (uint32_t)tile, (uint32_t)radix, (uint32_t)fused};
+      b->tuned[key] = p;
+      b->tuned_ms[key] = (float)ms;
+    }
+    pos = o1 + 1;
+  }
+}
+
 // Create the test's state on the device and add it to the active set.
 int admit(lnt_batch* b, uint64_t id, uint32_t exponent, uint32_t n, int prp, uint64_t iterations,
           Clock::time_point since) {
@@ -339,13 +430,17 @@ int admit(lnt_batch* b, uint64_t id, uint32_t exponent, uint32_t n, int prp, uin
     const uint64_t key = ((uint64_t)n << 8) | run;
     auto it = b->tuned.find(key);
     if (it == b->tuned.end()) {
-      lnt_plan_options tried[64];
-      float ms[64];
+      lnt_plan_options tried[128];
+      float ms[128];
       int count = 0, best = -1;
-      st = lnt_autotune(exponent, n, prp, b->device, b->tune_loops, tried, ms, 64, &count, &best);
+      st = lnt_autotune(exponent, n, prp, b->device, b->tune_loops, tried, ms, 128, &count, &best);
       lnt_plan_options chosen{};
-      if (st == LNT_OK && best >= 0 && best < 64) chosen = tried[best];
+      if (st == LNT_OK && best >= 0 && best < 128) {
+        chosen = tried[best];
+        b->tuned_ms[key] = ms[best];
+      }
       it = b->tuned.emplace(key, chosen).first;
+      if (!b->cache_path.empty()) save_plan_cache(b);
     }
     plan = &it->second;
   }
@@ -392,6 +487,28 @@ int admit_pending(lnt_batch* b) {
   return LNT_OK;
 }
 
+// Squarings a test may run before its target or its next checkpoint.
+uint64_t steps_left(const lnt_batch* b, const Entry& e) {
+  uint64_t r = e.target - e.done;
+  if (b->checkpoint_every) r = std::min(r, b->checkpoint_every - e.done % b->checkpoint_every);
+  return r;
+}
+
+// Res64 of every test that has just reached a checkpoint below its target.
+void record_checkpoints(lnt_batch* b) {
+  if (!b->checkpoint_every) return;
+  for (Entry& e : b->active) {
+    if (e.done == 0 || e.done >= e.target || e.done % b->checkpoint_every || e.last_checkpoint == e.done)
+      continue;
+    lnt_batch_checkpoint c{};
+    c.id = e.id;
+    c.iteration = e.done;
+    c.status = lnt_res64(e.t, &c.res64);
+    b->checkpoints.push_back(c);
+    e.last_checkpoint = e.done;
+  }
+}
+
 int check_request(uint32_t exponent, uint32_t& n) {
   if (n == 0) n = 1u << lnt_secured_log2_length(exponent);
   if (lnt::test_device_bytes(n) == 0) return berr(LNT_ERR_UNSUPPORTED_LENGTH, "unsupported length");
@@ -435,19 +552,25 @@ int lnt_batch_run(lnt_batch* b, uint64_t iterations) {
   DeviceGuard guard(b->device);
   int st = admit_pending(b);
   if (st != LNT_OK) return st;
+  record_checkpoints(b);  // tests admitted at a checkpoint (their first squaring runs at admission)
   if (b->active.empty() || iterations == 0) return LNT_OK;
   if (b->dirty && (st = rebuild(b)) != LNT_OK) return st;
-  // grouped tests advance in lockstep: no test of a group may pass its target
+  // squarings test i may run in this call: up to its target and its next checkpoint
+  std::vector<uint64_t> step(b->active.size());
+  for (size_t i = 0; i < b->active.size(); ++i) step[i] = std::min(iterations, steps_left(b, b->active[i]));
+  // grouped tests advance in lockstep: no test of a group may pass its target or checkpoint
   uint64_t k = iterations;
   for (auto& kv : b->groups)
-    for (size_t i : kv.second.members) k = std::min(k, b->active[i].target - b->active[i].done);
+    for (size_t i : kv.second.members) k = std::min(k, step[i]);
+  for (auto& kv : b->groups)
+    for (size_t i : kv.second.members) step[i] = k;
   // SMEM-resident tests: one launch, per-test counts, beside the groups
   if (!b->resident.empty()) {
     std::vector<lnt::ResidentDesc> h;
     uint32_t max_n = 0;
     for (size_t i : b->resident) {
       Entry& e = b->active[i];
-      h.push_back(lnt::test_resident_desc(e.t, std::min(iterations, e.target - e.done)));
+      h.push_back(lnt::test_resident_desc(e.t, step[i]));
       max_n = std::max(max_n, e.n);
     }
     BCUDA(cudaMemcpyAsync(b->d_rdescs, h.data(), h.size() * sizeof(lnt::ResidentDesc),
@@ -465,25 +588,20 @@ int lnt_batch_run(lnt_batch* b, uint64_t iterations) {
     if (left && (st = launch_groups(b, left)) != LNT_OK) return st;
   }
   for (size_t i : b->singles) {
-    Entry& e = b->active[i];
-    const uint64_t ki = std::min(iterations, e.target - e.done);
-    if ((st = lnt_iterate(e.t, ki)) != LNT_OK) return st;
+    if ((st = lnt_iterate(b->active[i].t, step[i])) != LNT_OK) return st;
   }
   BCUDA(cudaDeviceSynchronize(), "synchronize");
   for (size_t i : b->resident) {
-    Entry& e = b->active[i];
-    e.done += std::min(iterations, e.target - e.done);
-    lnt::test_mark_iterated(e.t);
+    b->active[i].done += step[i];
+    lnt::test_mark_iterated(b->active[i].t);
   }
   for (auto& kv : b->groups)
     for (size_t i : kv.second.members) {
-      b->active[i].done += k;
+      b->active[i].done += step[i];
       lnt::test_mark_iterated(b->active[i].t);
     }
-  for (size_t i : b->singles) {
-    Entry& e = b->active[i];
-    e.done += std::min(iterations, e.target - e.done);
-  }
+  for (size_t i : b->singles) b->active[i].done += step[i];
+  record_checkpoints(b);
   if ((st = retire_finished(b)) != LNT_OK) return st;
   return admit_pending(b);
 }
@@ -491,6 +609,30 @@ int lnt_batch_run(lnt_batch* b, uint64_t iterations) {
 int lnt_batch_autotune(lnt_batch* b, uint32_t loops) {
   if (!b) return berr(LNT_ERR_INVALID_ARGUMENT, "null batch");
   b->tune_loops = loops;
+  return LNT_OK;
+}
+
+int lnt_batch_checkpoint_every(lnt_batch* b, uint64_t every) {
+  if (!b) return berr(LNT_ERR_INVALID_ARGUMENT, "null batch");
+  b->checkpoint_every = every;
+  return LNT_OK;
+}
+
+int lnt_batch_poll_checkpoints(lnt_batch* b, lnt_batch_checkpoint* out, int cap, int* count) {
+  if (!b || !count || (cap > 0 && !out)) return berr(LNT_ERR_INVALID_ARGUMENT, "null argument");
+  int k = 0;
+  while (k < cap && !b->checkpoints.empty()) {
+    out[k++] = b->checkpoints.front();
+    b->checkpoints.pop_front();
+  }
+  *count = k;
+  return LNT_OK;
+}
+
+int lnt_batch_plan_cache(lnt_batch* b, const char* path) {
+  if (!b) return berr(LNT_ERR_INVALID_ARGUMENT, "null batch");
+  b->cache_path = path ? path : "";
+  if (!b->cache_path.empty()) load_plan_cache(b);
   return LNT_OK;
 }
 

@@ -30,6 +30,7 @@ struct Plan {
   uint32_t tile = 0;    // columns per column-pass CTA = words per carry run
   uint32_t ntiles = 0;  // n1 / tile
   bool fast = false;    // register-pass kernels (lnt_radix16.cu) instead of radix-2
+  uint32_t radix = 8;   // register-pass kernels: largest pass radix, 8 or 16
   // steady squarings use the carry-fused column kernel (col_inverse of one
   // squaring + col_forward of the next): from 2^19 words, where its tiles fill
   // the GPU (at n = 2^23: 244.6 us for the pair that takes 270.1 us as two
@@ -44,9 +45,11 @@ constexpr uint32_t kMaxLog2 = 26;  // (p - 1) / 192 holds 2^26: the largest IBDW
 
 // Explicit choices for make_plan (the C ABI's lnt_plan_options); 0 = policy.
 struct PlanOptions {
-  uint32_t kind = 0;       // 0 policy, 1 resident, 2 two-pass radix-16, 3 two-pass radix-2
+  uint32_t kind = 0;       // 0 policy, 1 resident, 2 two-pass register passes, 3 two-pass radix-2
   uint32_t log2_rows = 0;  // two-pass: log2 n2 (column length)
   uint32_t tile = 0;       // two-pass: words per carry run (4 or 8)
+  uint32_t radix = 0;      // register passes: largest pass radix, 8 or 16
+  uint32_t fused = 0;      // register passes: 1 carry-fused column kernel, 2 two plain launches
 };
 
 // The plan for an n-word residue of exponent q.  With opt == nullptr (or all
@@ -56,6 +59,17 @@ bool make_plan(uint32_t n, uint32_t exponent, const PlanOptions* opt, Plan& plan
                std::string* why = nullptr);
 // Every valid explicit plan for (n, q): the autotuner's candidates.
 std::vector<PlanOptions> plan_candidates(uint32_t n, uint32_t exponent);
+
+// ------------------------------------------------------------ device ----
+struct DeviceInfo {
+  int sms = 0;                   // streaming multiprocessors
+  int smem_per_sm = 0;           // shared memory per SM, bytes
+  int smem_per_block_optin = 0;  // largest dynamic shared memory a CTA may ask for
+};
+// The current device's properties (queried once per device, then cached).
+cudaError_t device_info(DeviceInfo& out);
+// Its SM count (148 on B200 if the query fails).
+uint32_t device_sms();
 
 // ------------------------------------------------------ resident kernel ----
 // One residue per CTA, state kept in shared memory for all iterations.
@@ -75,7 +89,9 @@ struct ResidentDesc {
 };
 
 size_t resident_smem_bytes(uint32_t n, uint32_t threads);
-uint32_t resident_threads(uint32_t n, uint32_t count);
+// threads per CTA: one per 4 words when the launch has fewer tests than the
+// device has SMs (latency), one per 8 otherwise (throughput)
+uint32_t resident_threads(uint32_t n, uint32_t count, uint32_t sms);
 cudaError_t launch_resident(const ResidentDesc* d_descs, uint32_t count, uint32_t max_n,
                             cudaStream_t stream);
 
@@ -110,6 +126,7 @@ struct TwoPassDesc {
   uint32_t* fuse;
   uint32_t n1, n2, log2n1, log2n2, tile, ntiles;
   uint32_t prp;
+  uint32_t radix;  // largest pass radix of the row and column transforms: 8 or 16
 };
 
 cudaError_t launch_col_forward(const TwoPassDesc& d, bool apply_carries, cudaStream_t s);
@@ -118,10 +135,9 @@ cudaError_t launch_col_inverse(const TwoPassDesc& d, bool unsigned_mode, cudaStr
 
 // radix-16 pass variants (lnt_radix16.cu): n2 in [2^6, 2^12], n1 in [2^7, 2^12], n1 >= n2
 bool r16_supported(uint32_t log2n1, uint32_t log2n2);
-// radices of the passes of a length-2^log2L transform, first (largest span) first,
-// and the largest radix the kernels were built with (8 or 16)
-std::vector<uint32_t> r16_pass_radices(uint32_t log2L);
-uint32_t r16_max_radix();
+// radices of the passes of a length-2^log2L transform whose passes take at most
+// `radix` (8 or 16) points, first (largest span) first
+std::vector<uint32_t> r16_pass_radices(uint32_t log2L, uint32_t radix);
 uint32_t r16_tile(uint32_t log2n2);
 uint32_t r16_run_words_needed(uint32_t exponent, uint32_t log2n);
 // `d` gives the geometry (shared by every test of the launch); `dd` is a device

@@ -6,8 +6,8 @@
 // cannot allocate device memory at the time they need a residue in the
 // reference's digit format: a serving process whose HBM is entirely handed to
 // its own pool or admission budget, a latency-critical step where cudaMalloc's
-// implicit device synchronisation is unacceptable, or a checkpoint taken from an
-// interrupt handler.  For them this entry point takes every buffer from the
+// implicit device synchronisation is unacceptable, or a checkpoint written by a
+// path that must not allocate (outside the allocator's reach).  For them this entry point takes every buffer from the
 // caller and keeps the scratch in one fixed array of device memory that belongs
 // to the library: g_noalloc_scratch below, sized for residues of up to
 // 2^24 words (about 2.5 MiB, held by every GPU that loads the library until the
@@ -49,7 +49,9 @@ std::mutex g_mutex;
 unsigned char* g_scratch_ptr[kMaxDevices] = {};
 
 // The device address of the scratch array on the current device (set-up on
-// the first call per device).
+// the first call per device).  The address is kept for the life of the process:
+// a cudaDeviceReset (or anything else that tears down the device's primary
+// context) invalidates it, and this entry point must not be called after one.
 cudaError_t scratch_on_current_device(unsigned char** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -100,8 +102,22 @@ extern "C" int lnt_canonicalize_noalloc(const int64_t* words, const uint8_t* wid
     return LNT_ERR_INVALID_ARGUMENT;
   }
   cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
+  cudaError_t e;
+  if (s != nullptr) {
+    // the scratch address is the current device's: the stream must be on it
+    int cur = 0, sdev = 0;
+    if ((e = cudaGetDevice(&cur)) != cudaSuccess || (e = cudaStreamGetDevice(s, &sdev)) != cudaSuccess) {
+      lnt::set_last_error(std::string("lnt_canonicalize_noalloc: ") + cudaGetErrorString(e));
+      return LNT_ERR_CUDA;
+    }
+    if (sdev != cur) {
+      lnt::set_last_error("lnt_canonicalize_noalloc: the stream belongs to device " + std::to_string(sdev) +
+                          ", the current device is " + std::to_string(cur));
+      return LNT_ERR_INVALID_ARGUMENT;
+    }
+  }
   unsigned char* base = nullptr;
-  cudaError_t e = scratch_on_current_device(&base);
+  e = scratch_on_current_device(&base);
   if (e != cudaSuccess) {
     lnt::set_last_error(std::string("lnt_canonicalize_noalloc: scratch set-up: ") +
                         cudaGetErrorString(e));
@@ -127,13 +143,18 @@ extern "C" int lnt_canonicalize_noalloc(const int64_t* words, const uint8_t* wid
   }
   noalloc_digit0_flag<<<1, 1, 0, s>>>(digits, c.flags);
   noalloc_fix_zero<<<(n + 255) / 256, 256, 0, s>>>(digits, widths, n, c.flags, prp, zero_start);
+  // the flag word comes back on the caller's stream (not the legacy stream,
+  // which would wait for every blocking stream of the device)
   uint32_t flags = 0;
-  if ((e = cudaGetLastError()) != cudaSuccess || (e = cudaStreamSynchronize(s)) != cudaSuccess ||
-      (e = cudaMemcpy(&flags, c.flags, sizeof(flags), cudaMemcpyDeviceToHost)) != cudaSuccess) {
+  if ((e = cudaGetLastError()) != cudaSuccess ||
+      (e = cudaMemcpyAsync(&flags, c.flags, sizeof(flags), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(s)) != cudaSuccess) {
     lnt::set_last_error(std::string("lnt_canonicalize_noalloc: ") + cudaGetErrorString(e));
     return LNT_ERR_CUDA;
   }
   if (flags & lnt::kCanonError) {
+    // `digits` is left partly written; lnt_get_digits of a test may still
+    // succeed on such words (it falls back to an exact carry on the host)
     lnt::set_last_error("lnt_canonicalize_noalloc: words too far from normalised digits");
     return LNT_ERR_NUMERIC;
   }

@@ -86,7 +86,8 @@ static void name_plan(Plan& plan) {
     return;
   }
   plan.name = "TWOPASS_" + std::to_string(plan.n2) + "x" + std::to_string(plan.n1) +
-              (plan.fast ? "_R" + std::to_string(r16_max_radix()) : std::string("_R2")) + "_T" + std::to_string(plan.tile);
+              (plan.fast ? "_R" + std::to_string(plan.radix) : std::string("_R2")) + "_T" +
+              std::to_string(plan.tile) + (plan.fused ? "_F" : "");
 }
 
 // Column tiles the kernels can stage: radix-16 columns of 4096 words only fit
@@ -106,13 +107,16 @@ bool make_plan(uint32_t n, uint32_t exponent, const PlanOptions* opt, Plan& plan
   PlanOptions o = opt ? *opt : PlanOptions();
   if (n < 2 || (n & (n - 1)) || n > (1u << kMaxLog2)) return reject("length must be 2^k, 1 <= k <= 26");
   if (o.kind > 3) return reject("unknown plan kind");
+  if (o.radix != 0 && o.radix != 8 && o.radix != 16) return reject("pass radix must be 8 or 16");
+  if (o.fused > 2) return reject("fused must be 0 (policy), 1 (fused) or 2 (two launches)");
   plan = Plan();
   plan.n = n;
   while ((1u << plan.log2n) < n) plan.log2n++;
   if (o.kind == 0) o.kind = plan.log2n <= kResidentMaxLog2 ? 1 : 0;
   if (o.kind == 1) {
     if (plan.log2n > kResidentMaxLog2) return reject("resident plan needs n <= 4096");
-    if (o.log2_rows || o.tile) return reject("resident plan takes no split or tile");
+    if (o.log2_rows || o.tile || o.radix || o.fused)
+      return reject("resident plan takes no split, tile, radix or fusion choice");
     plan.kind = PlanKind::Resident;
     name_plan(plan);
     return true;
@@ -130,6 +134,7 @@ bool make_plan(uint32_t n, uint32_t exponent, const PlanOptions* opt, Plan& plan
       o.kind = 3;
   }
   plan.fast = o.kind == 2;
+  if (!plan.fast && (o.radix || o.fused)) return reject("radix and fusion choices need the register-pass kernels");
   if (plan.fast) {
     if (l2 == 0) l2 = plan.log2n / 2 < 12 ? plan.log2n / 2 : 12;
     l1 = plan.log2n - l2;
@@ -162,7 +167,12 @@ bool make_plan(uint32_t n, uint32_t exponent, const PlanOptions* opt, Plan& plan
   plan.n2 = 1u << l2;
   plan.tile = tile;
   plan.ntiles = plan.n1 / plan.tile;
-  plan.fused = plan.fast && plan.log2n >= 19;
+  if (plan.fast) {
+    plan.radix = o.radix ? o.radix : 8;
+    // policy: the carry-fused column kernel from 2^19 words, where its tiles
+    // fill the GPU; the autotuner may choose either way at any length
+    plan.fused = o.fused ? o.fused == 1 : plan.log2n >= 19;
+  }
   name_plan(plan);
   return true;
 }
@@ -176,6 +186,10 @@ static PlanOptions options_of(const Plan& p) {
   o.kind = p.fast ? 2 : 3;
   o.log2_rows = p.log2n2;
   o.tile = p.tile;
+  if (p.fast) {
+    o.radix = p.radix;
+    o.fused = p.fused ? 1 : 2;
+  }
   return o;
 }
 
@@ -183,7 +197,9 @@ std::vector<PlanOptions> plan_candidates(uint32_t n, uint32_t exponent) {
   std::vector<PlanOptions> out;
   auto add = [&](const PlanOptions& o) {
     for (const PlanOptions& c : out)
-      if (c.kind == o.kind && c.log2_rows == o.log2_rows && c.tile == o.tile) return;
+      if (c.kind == o.kind && c.log2_rows == o.log2_rows && c.tile == o.tile && c.radix == o.radix &&
+          c.fused == o.fused)
+        return;
     out.push_back(o);
   };
   Plan plan;
@@ -192,18 +208,26 @@ std::vector<PlanOptions> plan_candidates(uint32_t n, uint32_t exponent) {
   if (plan.kind == PlanKind::Resident) return out;
   const bool r16 = plan.fast;
   for (uint32_t l2 = 1; l2 <= 12 && l2 < plan.log2n; ++l2)
-    for (uint32_t tile : {4u, 8u}) {
-      // radix-2 only where no radix-16 plan exists, with splits near square
-      PlanOptions o;
-      o.kind = r16 ? 2 : 3;
-      o.log2_rows = l2;
-      o.tile = tile;
-      Plan p;
-      if (!make_plan(n, exponent, &o, p)) continue;
-      const int skew = (int)p.log2n1 - (int)p.log2n2;
-      if (!r16 && (skew < 0 || skew > 3)) continue;
-      add(o);
-    }
+    for (uint32_t tile : {4u, 8u})
+      for (uint32_t radix : {8u, 16u})
+        for (uint32_t fused : {1u, 2u}) {
+          // radix-2 only where no register-pass plan exists, with splits near square
+          PlanOptions o;
+          o.kind = r16 ? 2 : 3;
+          o.log2_rows = l2;
+          o.tile = tile;
+          if (r16) {
+            o.radix = radix;
+            o.fused = fused;
+          } else if (radix != 8 || fused != 1) {
+            continue;
+          }
+          Plan p;
+          if (!make_plan(n, exponent, &o, p)) continue;
+          const int skew = (int)p.log2n1 - (int)p.log2n2;
+          if (!r16 && (skew < 0 || skew > 3)) continue;
+          add(o);
+        }
   return out;
 }
 

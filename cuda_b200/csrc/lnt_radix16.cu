@@ -113,7 +113,7 @@ __device__ void row_dit_pass(uint64_t* sm, int ld, int rows, int L, int span, ui
     row_dit_tasks<R, false>(sm, ld, rows, L, span, x, twi, itwL);
 }
 
-template <bool Forward>
+template <bool Forward, int MR>
 __device__ __forceinline__ void row_pass_r(int R, uint64_t* sm, int ld, int rows, int L, int span,
                                            uint64_t* x, const uint64_t* tw4, const uint64_t* twL) {
   switch (R) {
@@ -130,13 +130,15 @@ __device__ __forceinline__ void row_pass_r(int R, uint64_t* sm, int ld, int rows
       else row_dit_pass<8>(sm, ld, rows, L, span, x, tw4, twL);
       break;
     default:
-      if constexpr (Forward) row_dif_pass<kMaxRadix>(sm, ld, rows, L, span, x, tw4, twL);
-      else row_dit_pass<kMaxRadix>(sm, ld, rows, L, span, x, tw4, twL);
+      if constexpr (MR >= 16) {
+        if constexpr (Forward) row_dif_pass<16>(sm, ld, rows, L, span, x, tw4, twL);
+        else row_dit_pass<16>(sm, ld, rows, L, span, x, tw4, twL);
+      }
       break;
   }
 }
 
-template <int TH>
+template <int TH, int MR>
 __global__ void __launch_bounds__(TH, TH == 256 ? LNT_ROW_MIN_BLOCKS : 1024 / TH) row_square_r16(const TwoPassDesc* __restrict__ Ds, Passes P, int rows) {
   extern __shared__ __align__(16) uint64_t sm[];
   const TwoPassDesc& D = Ds[blockIdx.y];
@@ -145,16 +147,16 @@ __global__ void __launch_bounds__(TH, TH == 256 ? LNT_ROW_MIN_BLOCKS : 1024 / TH
   uint64_t* x = reinterpret_cast<uint64_t*>(D.x) + off;
   int span = L;
   for (int j = 0, seg = 0; j + 1 < P.m; ++j) {
-    row_pass_r<true>(P.radix[j], sm, ld, rows, L, span, x, D.twf + off, D.itw1 + seg);
+    row_pass_r<true, MR>(P.radix[j], sm, ld, rows, L, span, x, D.twf + off, D.itw1 + seg);
     seg += span;
     span /= P.radix[j];
     __syncthreads();
   }
-  pass_r<2>(P.radix[P.m - 1], sm, ld, rows, L, span, nullptr);
+  pass_r<2, MR>(P.radix[P.m - 1], sm, ld, rows, L, span, nullptr);
   __syncthreads();
   for (int j = P.m - 2; j >= 0; --j) {
     span *= P.radix[j];
-    row_pass_r<false>(P.radix[j], sm, ld, rows, L, span, x, D.twi + off,
+    row_pass_r<false, MR>(P.radix[j], sm, ld, rows, L, span, x, D.twi + off,
                       D.iitw1 + pass_table_offset(P, L, j));
     if (j) __syncthreads();
   }
@@ -164,7 +166,7 @@ __global__ void __launch_bounds__(TH, TH == 256 ? LNT_ROW_MIN_BLOCKS : 1024 / TH
 // after all forward passes, in the order the passes leave them, go back to x.
 // With col_forward before it this is the full transform of a residue, the
 // operand of a product (row_mul_r16).
-template <int TH>
+template <int TH, int MR>
 __global__ void __launch_bounds__(TH) row_forward_r16(const TwoPassDesc* __restrict__ Ds, Passes P, int rows) {
   extern __shared__ __align__(16) uint64_t sm[];
   const TwoPassDesc& D = Ds[blockIdx.y];
@@ -173,7 +175,7 @@ __global__ void __launch_bounds__(TH) row_forward_r16(const TwoPassDesc* __restr
   uint64_t* x = reinterpret_cast<uint64_t*>(D.x) + off;
   int span = L;
   for (int j = 0, seg = 0; j < P.m; ++j) {
-    row_pass_r<true>(P.radix[j], sm, ld, rows, L, span, x, D.twf + off, D.itw1 + seg);
+    row_pass_r<true, MR>(P.radix[j], sm, ld, rows, L, span, x, D.twf + off, D.itw1 + seg);
     seg += span;
     span /= P.radix[j];
     __syncthreads();
@@ -186,7 +188,7 @@ __global__ void __launch_bounds__(TH) row_forward_r16(const TwoPassDesc* __restr
 
 // row_square_r16 with the pointwise square replaced by the product with the
 // transformed rows F of another residue (row_forward_r16's output).
-template <int TH>
+template <int TH, int MR>
 __global__ void __launch_bounds__(TH) row_mul_r16(const TwoPassDesc* __restrict__ Ds, Passes P, int rows,
                                                   const uint64_t* __restrict__ F) {
   extern __shared__ __align__(16) uint64_t sm[];
@@ -196,16 +198,16 @@ __global__ void __launch_bounds__(TH) row_mul_r16(const TwoPassDesc* __restrict_
   uint64_t* x = reinterpret_cast<uint64_t*>(D.x) + off;
   int span = L;
   for (int j = 0, seg = 0; j + 1 < P.m; ++j) {
-    row_pass_r<true>(P.radix[j], sm, ld, rows, L, span, x, D.twf + off, D.itw1 + seg);
+    row_pass_r<true, MR>(P.radix[j], sm, ld, rows, L, span, x, D.twf + off, D.itw1 + seg);
     seg += span;
     span /= P.radix[j];
     __syncthreads();
   }
-  pass_r<3>(P.radix[P.m - 1], sm, ld, rows, L, span, F + off);
+  pass_r<3, MR>(P.radix[P.m - 1], sm, ld, rows, L, span, F + off);
   __syncthreads();
   for (int j = P.m - 2; j >= 0; --j) {
     span *= P.radix[j];
-    row_pass_r<false>(P.radix[j], sm, ld, rows, L, span, x, D.twi + off,
+    row_pass_r<false, MR>(P.radix[j], sm, ld, rows, L, span, x, D.twi + off,
                       D.iitw1 + pass_table_offset(P, L, j));
     if (j) __syncthreads();
   }
@@ -252,6 +254,16 @@ __device__ __forceinline__ void tile_load(uint64_t* sm, int ld, const int64_t* x
     }
   }
   asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+// HBM -> shared memory through L2 only (ld.global.cg): for a tile another CTA
+// of the same launch has just written.
+__device__ __forceinline__ void tile_load_cg(uint64_t* sm, int ld, const int64_t* x, int L, int T,
+                                             uint32_t n1, uint32_t c0) {
+  for (int idx = threadIdx.x; idx < T * L; idx += blockDim.x) {
+    const int r = idx / T, c = idx % T;
+    sm[c * ld + sw(r)] = (uint64_t)__ldcg(x + (size_t)r * n1 + c0 + c);
+  }
 }
 
 // shared memory -> HBM: as tile_load, four rounds per loop iteration so the
@@ -310,7 +322,7 @@ __device__ __forceinline__ void load_widths(const uint8_t* src, unsigned (&out)[
 // Carry-in from the run before each row's run, weight, forward column passes,
 // store.  The tile's digits are in `sm`.  `cg_carries`: read the carries from L2
 // (written by another CTA of the same launch).
-template <int T>
+template <int T, int MR>
 __device__ __forceinline__ void forward_tile(const TwoPassDesc& D, const Passes& P, uint64_t* sm,
                                              int ld, uint32_t t0, bool apply_carries, bool cg_carries,
                                              uint32_t& status) {
@@ -348,7 +360,7 @@ __device__ __forceinline__ void forward_tile(const TwoPassDesc& D, const Passes&
   __syncthreads();
   int span = L;
   for (int j = 0, seg = 0; j < P.m; ++j) {
-    pass_r<0>(P.radix[j], sm, ld, T, L, span, D.itw2 + seg);
+    pass_r<0, MR>(P.radix[j], sm, ld, T, L, span, D.itw2 + seg);
     seg += span;
     span /= P.radix[j];
     __syncthreads();
@@ -359,14 +371,14 @@ __device__ __forceinline__ void forward_tile(const TwoPassDesc& D, const Passes&
 // Inverse column passes, unweight, carry each row's run of T words to balanced
 // digits (minus two in the run of word 0), store the runs' outgoing carries.
 // The tile's transform is in `sm`; its digits are left there.
-template <int T>
+template <int T, int MR>
 __device__ __forceinline__ void inverse_tile(const TwoPassDesc& D, const Passes& P, uint64_t* sm,
                                              int ld, uint32_t t0, bool unsigned_mode) {
   const int L = (int)D.n2;
   int span = 1;
   for (int j = P.m - 1; j >= 0; --j) {
     span *= P.radix[j];
-    pass_r<1>(P.radix[j], sm, ld, T, L, span, D.iitw2 + pass_table_offset(P, L, j));
+    pass_r<1, MR>(P.radix[j], sm, ld, T, L, span, D.iitw2 + pass_table_offset(P, L, j));
     __syncthreads();
   }
   for (int r = threadIdx.x; r < L; r += blockDim.x) {
@@ -386,7 +398,7 @@ __device__ __forceinline__ void inverse_tile(const TwoPassDesc& D, const Passes&
   __syncthreads();
 }
 
-template <int T, int TH>
+template <int T, int TH, int MR>
 __global__ void __launch_bounds__(TH, TH == col_threads<T>() ? col_min_blocks<T>() : 1) col_forward_r16(
     const TwoPassDesc* __restrict__ Ds, Passes P, int apply_carries) {
   extern __shared__ __align__(16) uint64_t sm[];
@@ -395,11 +407,11 @@ __global__ void __launch_bounds__(TH, TH == col_threads<T>() ? col_min_blocks<T>
   uint32_t status = 0;
   tile_load(sm, ld, D.x, (int)D.n2, T, D.n1, blockIdx.x * T);
   __syncthreads();
-  forward_tile<T>(D, P, sm, ld, blockIdx.x, apply_carries != 0, false, status);
+  forward_tile<T, MR>(D, P, sm, ld, blockIdx.x, apply_carries != 0, false, status);
   if (status) atomicOr(D.status, status);
 }
 
-template <int T, int TH>
+template <int T, int TH, int MR>
 __global__ void __launch_bounds__(TH, TH == col_threads<T>() ? col_min_blocks<T>() : 1) col_inverse_r16(
     const TwoPassDesc* __restrict__ Ds, Passes P, int unsigned_mode) {
   extern __shared__ __align__(16) uint64_t sm[];
@@ -407,7 +419,7 @@ __global__ void __launch_bounds__(TH, TH == col_threads<T>() ? col_min_blocks<T>
   const int ld = col_ld((int)D.n2, T);
   tile_load(sm, ld, D.x, (int)D.n2, T, D.n1, blockIdx.x * T);
   __syncthreads();
-  inverse_tile<T>(D, P, sm, ld, blockIdx.x, unsigned_mode != 0);
+  inverse_tile<T, MR>(D, P, sm, ld, blockIdx.x, unsigned_mode != 0);
   tile_store(sm, ld, D.x, (int)D.n2, T, D.n1, blockIdx.x * T);
 }
 
@@ -415,15 +427,21 @@ __global__ void __launch_bounds__(TH, TH == col_threads<T>() ? col_min_blocks<T>
 // of the next in one launch, the tile staying in shared memory in between.
 //
 // A tile's second half needs the carries of the tile before it (the runs of
-// the same rows).  CTAs take tiles in ticket order (an atomic counter), so the
-// CTA of tile t - 1 has started before the CTA of tile t; every tile publishes
-// its carries with a release flag right after its first half, which waits for
-// nothing, and tile t waits only for tile t - 1's flag.  Tile 0 needs the LAST
-// tile's carries: its CTA waits for the last ticket.  That cannot deadlock:
-// every other CTA waits only for a CTA that is already running, so CTAs keep
-// finishing and the last tile gets a slot; tile 0's second half then runs
-// beside the last tile's.  Flags hold a per-launch epoch, so nothing is
-// cleared between launches.  Every wait is bounded in time and reported.
+// the same rows); tile 0 needs those of the LAST tile (the runs of the rows
+// before).  CTAs take tickets in start order (an atomic counter) and no CTA
+// ever waits for a CTA that took a later ticket, so every wait ends whatever
+// else holds the GPU's CTA slots (other tests, other launches):
+//   ticket 0:          first half of the last tile (its digits go back to x,
+//                      flag), first half of tile 0 (flag), then tile 0's
+//                      second half with the last tile's carries it has just
+//                      made itself;
+//   ticket t, 0<t<T-1: first half of tile t (flag), wait for tile t-1's flag,
+//                      second half;
+//   ticket T-1:        wait for the last tile's flag (ticket 0 has stored its
+//                      digits) and tile T-2's flag, reload the digits, second
+//                      half.
+// Flags hold a per-launch epoch, so nothing is cleared between launches.  Every
+// wait is bounded in time and reported.
 //
 // fuse[0]: ticket counter, fuse[1]: epoch, fuse[2 + t]: flag of tile t.
 constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s: far above any launch; then report, never hang
@@ -464,14 +482,14 @@ __device__ __forceinline__ void wait_flag(const uint32_t* flag, uint32_t want, u
   __syncthreads();
 }
 
-template <int T, int TH>
+template <int T, int TH, int MR>
 __global__ void __launch_bounds__(TH, TH == col_threads<T>() ? col_min_blocks<T>() : 1) col_fused_r16(
     const TwoPassDesc* __restrict__ Ds, Passes P) {
   extern __shared__ __align__(16) uint64_t sm[];
   __shared__ uint32_t s_ticket, s_epoch;
   const TwoPassDesc& D = Ds[blockIdx.y];
   const int L = (int)D.n2, ld = col_ld(L, T);
-  const uint32_t n1 = D.n1, ntiles = D.ntiles;
+  const uint32_t n1 = D.n1, ntiles = D.ntiles, last = ntiles - 1;
   uint32_t* ctl = D.fuse;
   if (threadIdx.x == 0) {
     // the epoch is read before the ticket: the last ticket's CTA advances it
@@ -482,28 +500,44 @@ __global__ void __launch_bounds__(TH, TH == col_threads<T>() ? col_min_blocks<T>
     s_ticket = atomicAdd(ctl, 1u);
   }
   __syncthreads();
-  const uint32_t t0 = s_ticket, ready = s_epoch + 1;
-  if (t0 >= ntiles) {  // a counter left over from a launch that did not finish: report, touch nothing
+  const uint32_t ticket = s_ticket, ready = s_epoch + 1;
+  if (ticket >= ntiles || ntiles < 2) {  // a counter left over from a launch that did not finish: report, touch nothing
     if (threadIdx.x == 0) atomicOr(D.status, kStatusFuseTimeout);
     return;
   }
   uint32_t status = 0;
 
-  // first half: inverse column transform of tile t0, carries out
-  tile_load(sm, ld, D.x, L, T, n1, t0 * T);
-  __syncthreads();
-  inverse_tile<T>(D, P, sm, ld, t0, false);
-  publish_flag(ctl + 2 + t0, ready);
-
-  // second half: carries in from the tile before (tile 0: the last tile),
-  // weight, forward column transform
-  wait_flag(ctl + 2 + (t0 > 0 ? t0 - 1 : ntiles - 1), ready, D.status);
-  forward_tile<T>(D, P, sm, ld, t0, true, true, status);
-  if (t0 == ntiles - 1 && threadIdx.x == 0) {
-    // every ticket of this launch is taken and every CTA has read the epoch
-    ctl[0] = 0;
-    __threadfence();
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(ctl + 1), "r"(ready) : "memory");
+  if (ticket == last) {
+    // the last tile's first half was done by ticket 0 (digits in x)
+    wait_flag(ctl + 2 + last, ready, D.status);
+    tile_load_cg(sm, ld, D.x, L, T, n1, last * T);
+    wait_flag(ctl + 2 + last - 1, ready, D.status);
+    forward_tile<T, MR>(D, P, sm, ld, last, true, true, status);
+    if (threadIdx.x == 0) {
+      // every ticket of this launch is taken and every CTA has read the epoch
+      ctl[0] = 0;
+      __threadfence();
+      asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(ctl + 1), "r"(ready) : "memory");
+    }
+  } else {
+    if (ticket == 0) {
+      // first half of the last tile: its carries feed tile 0 below, its
+      // digits wait in x for the last ticket
+      tile_load(sm, ld, D.x, L, T, n1, last * T);
+      __syncthreads();
+      inverse_tile<T, MR>(D, P, sm, ld, last, false);
+      tile_store(sm, ld, D.x, L, T, n1, last * T);
+      publish_flag(ctl + 2 + last, ready);
+    }
+    // first half: inverse column transform of the tile, carries out
+    tile_load(sm, ld, D.x, L, T, n1, ticket * T);
+    __syncthreads();
+    inverse_tile<T, MR>(D, P, sm, ld, ticket, false);
+    publish_flag(ctl + 2 + ticket, ready);
+    // second half: carries in from the tile before (tile 0: the last tile,
+    // made by this CTA), weight, forward column transform
+    if (ticket > 0) wait_flag(ctl + 2 + ticket - 1, ready, D.status);
+    forward_tile<T, MR>(D, P, sm, ld, ticket, true, true, status);
   }
   if (status) atomicOr(D.status, status);
 }
@@ -530,16 +564,15 @@ cudaError_t ensure_smem(K* kernel, size_t smem) {
 int row_rows_per_cta(int L, int n2) {
   int rows = 4096 / L;
   if (rows < 1) rows = 1;
-  while (rows > 1 && n2 / rows < 148) rows /= 2;
+  const int sms = (int)device_sms();
+  while (rows > 1 && n2 / rows < sms) rows /= 2;
   return rows;
 }
 
 }  // namespace
 
-uint32_t r16_max_radix() { return (uint32_t)kMaxRadix; }
-
-std::vector<uint32_t> r16_pass_radices(uint32_t log2L) {
-  const Passes p = make_passes((int)log2L);
+std::vector<uint32_t> r16_pass_radices(uint32_t log2L, uint32_t radix) {
+  const Passes p = make_passes((int)log2L, radix == 16 ? 4 : 3);
   std::vector<uint32_t> r;
   for (int j = 0; j < p.m; ++j) r.push_back((uint32_t)p.radix[j]);
   return r;
@@ -565,131 +598,171 @@ uint32_t r16_run_words_needed(uint32_t exponent, uint32_t log2n) {
   return (log2n + wmax + wmin - 2) / (wmin - 1) + 1;
 }
 
-template <int TH>
+// log2 of the largest pass radix of a descriptor's plan (3: radix 8, 4: radix 16)
+inline int radix_log2(const TwoPassDesc& d) { return d.radix == 16 ? 4 : 3; }
+
+template <int TH, int MR>
 cudaError_t row_square_t(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count, cudaStream_t s) {
   const int L = (int)d.n1, rows = row_rows_per_cta(L, (int)d.n2);
   const size_t smem = (size_t)rows * padded(L) * 8;
-  cudaError_t e = ensure_smem(row_square_r16<TH>, smem);
+  cudaError_t e = ensure_smem(row_square_r16<TH, MR>, smem);
   if (e != cudaSuccess) return e;
-  row_square_r16<TH><<<dim3(d.n2 / rows, count), TH, smem, s>>>(dd, make_passes((int)d.log2n1), rows);
+  row_square_r16<TH, MR><<<dim3(d.n2 / rows, count), TH, smem, s>>>(
+      dd, make_passes((int)d.log2n1, radix_log2(d)), rows);
   return cudaGetLastError();
 }
 
-template <int TH>
+template <int TH, int MR>
 cudaError_t row_forward_t(const TwoPassDesc& d, const TwoPassDesc* dd, cudaStream_t s) {
   const int L = (int)d.n1, rows = row_rows_per_cta(L, (int)d.n2);
   const size_t smem = (size_t)rows * padded(L) * 8;
-  cudaError_t e = ensure_smem(row_forward_r16<TH>, smem);
+  cudaError_t e = ensure_smem(row_forward_r16<TH, MR>, smem);
   if (e != cudaSuccess) return e;
-  row_forward_r16<TH><<<dim3(d.n2 / rows, 1), TH, smem, s>>>(dd, make_passes((int)d.log2n1), rows);
+  row_forward_r16<TH, MR><<<dim3(d.n2 / rows, 1), TH, smem, s>>>(
+      dd, make_passes((int)d.log2n1, radix_log2(d)), rows);
   return cudaGetLastError();
 }
 
-template <int TH>
+template <int TH, int MR>
 cudaError_t row_mul_t(const TwoPassDesc& d, const TwoPassDesc* dd, const uint64_t* F, cudaStream_t s) {
   const int L = (int)d.n1, rows = row_rows_per_cta(L, (int)d.n2);
   const size_t smem = (size_t)rows * padded(L) * 8;
-  cudaError_t e = ensure_smem(row_mul_r16<TH>, smem);
+  cudaError_t e = ensure_smem(row_mul_r16<TH, MR>, smem);
   if (e != cudaSuccess) return e;
-  row_mul_r16<TH><<<dim3(d.n2 / rows, 1), TH, smem, s>>>(dd, make_passes((int)d.log2n1), rows, F);
+  row_mul_r16<TH, MR><<<dim3(d.n2 / rows, 1), TH, smem, s>>>(
+      dd, make_passes((int)d.log2n1, radix_log2(d)), rows, F);
   return cudaGetLastError();
 }
 
-cudaError_t launch_row_forward_r16(const TwoPassDesc& d, const TwoPassDesc* dd, cudaStream_t s) {
+template <int MR>
+cudaError_t row_forward_m(const TwoPassDesc& d, const TwoPassDesc* dd, cudaStream_t s) {
   switch (row_threads_for((int)d.n1)) {
-    case 256: return row_forward_t<256>(d, dd, s);
-    case 512: return row_forward_t<512>(d, dd, s);
-    default: return row_forward_t<1024>(d, dd, s);
+    case 256: return row_forward_t<256, MR>(d, dd, s);
+    case 512: return row_forward_t<512, MR>(d, dd, s);
+    default: return row_forward_t<1024, MR>(d, dd, s);
   }
+}
+
+template <int MR>
+cudaError_t row_mul_m(const TwoPassDesc& d, const TwoPassDesc* dd, const uint64_t* F, cudaStream_t s) {
+  switch (row_threads_for((int)d.n1)) {
+    case 256: return row_mul_t<256, MR>(d, dd, F, s);
+    case 512: return row_mul_t<512, MR>(d, dd, F, s);
+    default: return row_mul_t<1024, MR>(d, dd, F, s);
+  }
+}
+
+template <int MR>
+cudaError_t row_square_m(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count, cudaStream_t s) {
+  switch (row_threads_for((int)d.n1)) {
+    case 256: return row_square_t<256, MR>(d, dd, count, s);
+    case 512: return row_square_t<512, MR>(d, dd, count, s);
+    default: return row_square_t<1024, MR>(d, dd, count, s);
+  }
+}
+
+cudaError_t launch_row_forward_r16(const TwoPassDesc& d, const TwoPassDesc* dd, cudaStream_t s) {
+  return d.radix == 16 ? row_forward_m<16>(d, dd, s) : row_forward_m<8>(d, dd, s);
 }
 
 cudaError_t launch_row_mul_r16(const TwoPassDesc& d, const TwoPassDesc* dd, const uint64_t* F,
                                cudaStream_t s) {
-  switch (row_threads_for((int)d.n1)) {
-    case 256: return row_mul_t<256>(d, dd, F, s);
-    case 512: return row_mul_t<512>(d, dd, F, s);
-    default: return row_mul_t<1024>(d, dd, F, s);
-  }
+  return d.radix == 16 ? row_mul_m<16>(d, dd, F, s) : row_mul_m<8>(d, dd, F, s);
 }
 
 cudaError_t launch_row_square_r16(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
                                   cudaStream_t s) {
-  switch (row_threads_for((int)d.n1)) {
-    case 256: return row_square_t<256>(d, dd, count, s);
-    case 512: return row_square_t<512>(d, dd, count, s);
-    default: return row_square_t<1024>(d, dd, count, s);
-  }
+  return d.radix == 16 ? row_square_m<16>(d, dd, count, s) : row_square_m<8>(d, dd, count, s);
 }
 
 // Columns of 4096 words hold one CTA per SM: 1024 threads instead of 128 per column.
 template <int T>
 constexpr int col_wide_threads() { return 1024; }
 
-template <int T, int TH>
+template <int T, int TH, int MR>
 cudaError_t col_forward_t(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count, bool apply,
                           cudaStream_t s) {
   const size_t smem = (size_t)T * col_ld((int)d.n2, T) * 8;
-  cudaError_t e = ensure_smem(col_forward_r16<T, TH>, smem);
+  cudaError_t e = ensure_smem(col_forward_r16<T, TH, MR>, smem);
   if (e != cudaSuccess) return e;
-  col_forward_r16<T, TH><<<dim3(d.ntiles, count), TH, smem, s>>>(dd, make_passes((int)d.log2n2),
-                                                                  apply ? 1 : 0);
+  col_forward_r16<T, TH, MR><<<dim3(d.ntiles, count), TH, smem, s>>>(
+      dd, make_passes((int)d.log2n2, radix_log2(d)), apply ? 1 : 0);
   return cudaGetLastError();
 }
 
-template <int T, int TH>
+template <int T, int TH, int MR>
 cudaError_t col_inverse_t(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
                           bool unsigned_mode, cudaStream_t s) {
   const size_t smem = (size_t)T * col_ld((int)d.n2, T) * 8;
-  cudaError_t e = ensure_smem(col_inverse_r16<T, TH>, smem);
+  cudaError_t e = ensure_smem(col_inverse_r16<T, TH, MR>, smem);
   if (e != cudaSuccess) return e;
-  col_inverse_r16<T, TH><<<dim3(d.ntiles, count), TH, smem, s>>>(dd, make_passes((int)d.log2n2),
-                                                                  unsigned_mode ? 1 : 0);
+  col_inverse_r16<T, TH, MR><<<dim3(d.ntiles, count), TH, smem, s>>>(
+      dd, make_passes((int)d.log2n2, radix_log2(d)), unsigned_mode ? 1 : 0);
   return cudaGetLastError();
 }
 
-template <int T, int TH>
+template <int T, int TH, int MR>
 cudaError_t col_fused_t(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count, cudaStream_t s) {
   const size_t smem = (size_t)T * col_ld((int)d.n2, T) * 8;
-  cudaError_t e = ensure_smem(col_fused_r16<T, TH>, smem);
+  cudaError_t e = ensure_smem(col_fused_r16<T, TH, MR>, smem);
   if (e != cudaSuccess) return e;
-  col_fused_r16<T, TH><<<dim3(d.ntiles, count), TH, smem, s>>>(dd, make_passes((int)d.log2n2));
+  col_fused_r16<T, TH, MR><<<dim3(d.ntiles, count), TH, smem, s>>>(
+      dd, make_passes((int)d.log2n2, radix_log2(d)));
   return cudaGetLastError();
 }
 
-// Each test of a launch keeps its tile-0 CTA resident while it waits for the
-// test's last tile; at most 128 tests per launch leave most of the GPU's
-// (at least 148) CTA slots to the CTAs those waits depend on, whatever order
-// the hardware dispatches CTAs in.
-constexpr uint32_t kFusedTestsPerLaunch = 128;
+// Tests per launch (the grid's y extent).  A CTA of the fused kernel waits only
+// for CTAs that started before it, so the count is not bounded by how many
+// CTAs the GPU holds at once.
+constexpr uint32_t kFusedTestsPerLaunch = 1024;
 
-cudaError_t launch_col_fused_r16(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
-                                 cudaStream_t s) {
+template <int MR>
+cudaError_t col_fused_m(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count, cudaStream_t s) {
   for (uint32_t first = 0; first < count; first += kFusedTestsPerLaunch) {
     const uint32_t c = count - first < kFusedTestsPerLaunch ? count - first : kFusedTestsPerLaunch;
     cudaError_t e;
     if (d.tile == 8)
-      e = col_fused_t<8, col_threads<8>()>(d, dd + first, c, s);
+      e = col_fused_t<8, col_threads<8>(), MR>(d, dd + first, c, s);
     else if (d.n2 >= 4096)
-      e = col_fused_t<4, col_wide_threads<4>()>(d, dd + first, c, s);
+      e = col_fused_t<4, col_wide_threads<4>(), MR>(d, dd + first, c, s);
     else
-      e = col_fused_t<4, col_threads<4>()>(d, dd + first, c, s);
+      e = col_fused_t<4, col_threads<4>(), MR>(d, dd + first, c, s);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
 }
 
+template <int MR>
+cudaError_t col_forward_m(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count, bool apply,
+                          cudaStream_t s) {
+  if (d.tile == 8) return col_forward_t<8, col_threads<8>(), MR>(d, dd, count, apply, s);
+  if (d.n2 >= 4096) return col_forward_t<4, col_wide_threads<4>(), MR>(d, dd, count, apply, s);
+  return col_forward_t<4, col_threads<4>(), MR>(d, dd, count, apply, s);
+}
+
+template <int MR>
+cudaError_t col_inverse_m(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
+                          bool unsigned_mode, cudaStream_t s) {
+  if (d.tile == 8) return col_inverse_t<8, col_threads<8>(), MR>(d, dd, count, unsigned_mode, s);
+  if (d.n2 >= 4096) return col_inverse_t<4, col_wide_threads<4>(), MR>(d, dd, count, unsigned_mode, s);
+  return col_inverse_t<4, col_threads<4>(), MR>(d, dd, count, unsigned_mode, s);
+}
+
+cudaError_t launch_col_fused_r16(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
+                                 cudaStream_t s) {
+  return d.radix == 16 ? col_fused_m<16>(d, dd, count, s) : col_fused_m<8>(d, dd, count, s);
+}
+
 cudaError_t launch_col_forward_r16(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
                                    bool apply, cudaStream_t s) {
-  if (d.tile == 8) return col_forward_t<8, col_threads<8>()>(d, dd, count, apply, s);
-  if (d.n2 >= 4096) return col_forward_t<4, col_wide_threads<4>()>(d, dd, count, apply, s);
-  return col_forward_t<4, col_threads<4>()>(d, dd, count, apply, s);
+  return d.radix == 16 ? col_forward_m<16>(d, dd, count, apply, s)
+                       : col_forward_m<8>(d, dd, count, apply, s);
 }
 
 cudaError_t launch_col_inverse_r16(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
                                    bool unsigned_mode, cudaStream_t s) {
-  if (d.tile == 8) return col_inverse_t<8, col_threads<8>()>(d, dd, count, unsigned_mode, s);
-  if (d.n2 >= 4096) return col_inverse_t<4, col_wide_threads<4>()>(d, dd, count, unsigned_mode, s);
-  return col_inverse_t<4, col_threads<4>()>(d, dd, count, unsigned_mode, s);
+  return d.radix == 16 ? col_inverse_m<16>(d, dd, count, unsigned_mode, s)
+                       : col_inverse_m<8>(d, dd, count, unsigned_mode, s);
 }
 
 }  // namespace lnt

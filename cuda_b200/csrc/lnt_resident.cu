@@ -13,6 +13,9 @@
 // carry -> minus two run back to back inside one launch for all iterations, so
 // the loop is bound by the SM's integer pipe, not by launch latency.  Many
 // residues (a batch) run as many CTAs of the same launch.
+#include <mutex>
+#include <set>
+
 #include "lnt_internal.h"
 #include "carry.cuh"
 #include "smem_passes.cuh"
@@ -114,8 +117,8 @@ __global__ void __launch_bounds__(kMaxThreads) resident_square_loop(const Reside
 
 }  // namespace
 
-uint32_t resident_threads(uint32_t n, uint32_t count) {
-  uint32_t t = n / (count < 148 ? 4u : 8u);
+uint32_t resident_threads(uint32_t n, uint32_t count, uint32_t sms) {
+  uint32_t t = n / (count < sms ? 4u : 8u);
   t = t < 32 ? 32 : t;
   return t > kMaxThreads ? kMaxThreads : t;
 }
@@ -126,28 +129,37 @@ size_t resident_smem_bytes(uint32_t n, uint32_t threads) {
 
 cudaError_t launch_resident(const ResidentDesc* d_descs, uint32_t count, uint32_t max_n,
                             cudaStream_t stream) {
-  const uint32_t threads = resident_threads(max_n, count);
+  DeviceInfo info;
+  cudaError_t e = device_info(info);
+  if (e != cudaSuccess) return e;
+  const uint32_t sms = (uint32_t)info.sms;
+  const uint32_t threads = resident_threads(max_n, count, sms);
   size_t smem = resident_smem_bytes(max_n, threads);
   // Fewer tests than SMs: every test gets an SM of its own.  Left to itself
   // the block scheduler may place two of the CTAs on one SM (their registers
   // and shared memory fit), which halves both tests' speed while other SMs
   // idle; a CTA holding more than half of an SM's shared memory cannot share.
-  int dev = 0, sms = 0, per_sm = 0, per_block = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (e == cudaSuccess)
-    e = cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
-  if (e == cudaSuccess)
-    e = cudaDeviceGetAttribute(&per_block, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  if (e != cudaSuccess) return e;
-  if (count > 1 && count <= (uint32_t)sms) {
-    const size_t solo = (size_t)per_sm / 2 + 1024;
-    if (solo > smem && solo <= (size_t)per_block) smem = solo;
+  if (count > 1 && count <= sms) {
+    const size_t solo = (size_t)info.smem_per_sm / 2 + 1024;
+    if (solo > smem && solo <= (size_t)info.smem_per_block_optin) smem = solo;
   }
-  e = cudaFuncSetAttribute(resident_square_loop,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  resident_square_loop<<<count, threads, smem, stream>>>(d_descs, count < 148 ? 1 : 0);
+  // the kernel's dynamic shared-memory cap, raised once per device to the
+  // largest a launch can ask for
+  {
+    static std::mutex mu;
+    static std::set<int> raised;
+    int dev = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!raised.count(dev)) {
+      e = cudaFuncSetAttribute(resident_square_loop, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               info.smem_per_block_optin);
+      if (e != cudaSuccess) return e;
+      raised.insert(dev);
+    }
+  }
+  if (smem > (size_t)info.smem_per_block_optin) return cudaErrorInvalidValue;
+  resident_square_loop<<<count, threads, smem, stream>>>(d_descs, count < sms ? 1 : 0);
   return cudaGetLastError();
 }
 

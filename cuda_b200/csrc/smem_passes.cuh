@@ -33,17 +33,17 @@ struct Passes {
   int radix[6];   // r_0 (largest stride) ... r_{m-1} (contiguous)
 };
 
-// Largest pass radix.  8 (three radix-2 stages per pass) keeps a task's values,
-// twiddles and addresses within the 64 registers that four row CTAs (two column
-// CTAs) per SM allow; 16 needs one twiddle stage less per direction but spills
-// (measured at n = 2^23: 561 us per squaring with 8, 574 with 16).
-#ifndef LNT_MAX_RADIX_LOG2
-#define LNT_MAX_RADIX_LOG2 3
-#endif
-constexpr int kMaxRadix = 1 << LNT_MAX_RADIX_LOG2;
+// Default largest pass radix.  8 (three radix-2 stages per pass) keeps a task's
+// values, twiddles and addresses within the 64 registers that four row CTAs
+// (two column CTAs) per SM allow; 16 needs one twiddle stage less per direction
+// but spills there.  The two-pass kernels are built for both (a plan's `radix`)
+// and the autotuner picks per length; the resident kernel uses 8.
+constexpr int kDefaultRadixLog2 = 3;
+constexpr int kMaxRadix = 1 << kDefaultRadixLog2;
 
-__host__ __device__ inline Passes make_passes(int log2L) {
-  constexpr int b = LNT_MAX_RADIX_LOG2;
+// Passes of a length-2^log2L transform with radices of at most 2^b: the first
+// pass takes the remainder, every later pass 2^b.
+__host__ __device__ inline Passes make_passes(int log2L, int b = kDefaultRadixLog2) {
   Passes p{};
   int first = log2L % b;
   int rest = log2L - first;
@@ -191,14 +191,17 @@ __device__ void pass(uint64_t* sm, int ld, int ntrans, int L, int span, const ui
     pass_tasks<R, Mode, false>(sm, ld, ntrans, L, span, tw);
 }
 
-template <int Mode>
+// A pass of radix R (a power of two up to MR, the largest the kernel is built for).
+template <int Mode, int MR = kMaxRadix>
 __device__ __forceinline__ void pass_r(int R, uint64_t* sm, int ld, int ntrans, int L, int span,
                                        const uint64_t* tw) {
   switch (R) {
     case 2: pass<2, Mode>(sm, ld, ntrans, L, span, tw); break;
     case 4: pass<4, Mode>(sm, ld, ntrans, L, span, tw); break;
     case 8: pass<8, Mode>(sm, ld, ntrans, L, span, tw); break;
-    default: pass<kMaxRadix, Mode>(sm, ld, ntrans, L, span, tw); break;
+    default:
+      if constexpr (MR >= 16) pass<16, Mode>(sm, ld, ntrans, L, span, tw);
+      break;
   }
 }
 

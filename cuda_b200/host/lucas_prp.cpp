@@ -79,7 +79,7 @@ void LucasPRP::Run() {
   } else {
     InitializeTest();
   }
-  EnableGerbicz();
+  EnableChecks();
   const Clock::time_point t0 = Clock::now();
   MainLoop();
   Check(lnt_synchronize(t_), "lnt_synchronize");
@@ -107,9 +107,22 @@ void LucasPRP::Run() {
   if (o_.dump_stats) DumpStats(total_ms_);
 }
 
-// The Gerbicz-Li check (GerbiczBlock, an extension) on the residue the loop
+// The error checks (extensions): the Gerbicz-Li check of PRP tests
+// (GerbiczBlock) or the Jacobi check of LL tests (JacobiCheck), on the residue the loop
 // starts from: a fresh test or the residue a resume loaded.
-void LucasPRP::EnableGerbicz() {
+void LucasPRP::EnableChecks() {
+  if (!o_.prp && o_.jacobi_interval) {
+    // the Jacobi check of LL tests (JacobiCheck, an extension): the symbol is
+    // defined from the first squaring on, so the check starts from the residue
+    // the loop begins with (a fresh start or a resumed one)
+    const int st = lnt_jacobi_enable(t_, o_.jacobi_interval);
+    jacobi_ = st == LNT_OK;
+    if (jacobi_)
+      LOG_VERBOSE("Jacobi check every %llu squarings", (unsigned long long)o_.jacobi_interval);
+    else
+      LOG_NORMAL("Jacobi check not available for this test: %s", lnt_last_error());
+    return;
+  }
   if (!o_.prp || o_.gerbicz_block == 0) return;
   const int st = lnt_gerbicz_enable(t_, o_.gerbicz_block);
   gerbicz_ = st == LNT_OK;
@@ -244,6 +257,8 @@ void LucasPRP::DumpStats(double total_ms) {
   r.res64 = res64_of(host_x_, widths_);
   if (gerbicz_ && lnt_gerbicz_stats(t_, nullptr, &r.gerbicz_checks, &r.gerbicz_errors) == LNT_OK)
     r.has_gerbicz = true;
+  if (jacobi_ && lnt_jacobi_stats(t_, nullptr, &r.jacobi_checks, &r.jacobi_errors) == LNT_OK)
+    r.has_jacobi = true;
   if (!WriteStatsFile(o_.stat_filename, r))
     LOG_NORMAL("Cannot write the statistics to %s", o_.stat_filename.c_str());
 }

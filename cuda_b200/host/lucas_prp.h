@@ -44,7 +44,7 @@ class LucasPRP : public Process {
   void DumpStats(double total_ms);
   void DumpEnvironment();
   void Check(int status, const char* what);
-  void EnableGerbicz();
+  void EnableChecks();
 
   MainOptions& o_;
   lnt_plan_options plan_;
@@ -59,6 +59,7 @@ class LucasPRP : public Process {
   double total_ms_ = 0;
   double ms_per_iteration_estimate_ = 0;
   bool gerbicz_ = false;
+  bool jacobi_ = false;
 };
 
 }  // namespace lucasntt

@@ -67,12 +67,12 @@ MainProcess::MainProcess(int argc, char** argv) {
   }
 
   // candidate plans of this length (the reference's candidate lengths x pools)
-  std::vector<lnt_plan_options> plans(64);
+  std::vector<lnt_plan_options> plans(128);
   int count = 0;
   const int st = lnt_plan_candidates(o_.exponent, n_, plans.data(), (int)plans.size(), &count);
   if (st != LNT_OK)
     throw std::runtime_error(std::string("No plan for this length: ") + lnt_last_error());
-  plans.resize((size_t)std::min(count, 64));
+  plans.resize((size_t)std::min(count, 128));
   std::vector<lnt_plan_options> chosen;
   const std::string& pool = o_.preferred_pool;
   if (!pool.empty()) {

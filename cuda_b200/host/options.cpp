@@ -50,6 +50,8 @@ MainOptions ResolveOptions(int argc, char** argv, const std::string& ini_path) {
   {
     const long b = ini ? ini->GetLongValue("GerbiczBlock", 0) : 0;
     o.gerbicz_block = b > 0 && b < (1L << 20) ? (uint32_t)b : 0;
+    const long j = ini ? ini->GetLongValue("JacobiCheck", 0) : 0;
+    o.jacobi_interval = j > 0 ? (uint64_t)j : 0;
   }
 
   // an interrupted run's stats file replaces LucasNTT.ini (main_process.cu:98-106)

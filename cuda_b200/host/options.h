@@ -37,6 +37,9 @@ struct MainOptions {
   // Extension: GerbiczBlock = B turns on the Gerbicz-Li check of PRP tests
   // (lnt_gerbicz_enable; a verification every B^2 squarings).  0 = off.
   uint32_t gerbicz_block = 0;
+  // Extension: JacobiCheck = K turns on the Jacobi check of LL tests
+  // (lnt_jacobi_enable; the symbol of the residue every K squarings).  0 = off.
+  uint64_t jacobi_interval = 0;
 };
 
 // Resolve the options.  `ini_path` is LucasNTT.ini in the working directory

@@ -111,6 +111,10 @@ bool WriteStatsFile(const std::string& path, const StatsRecord& r) {
     std::fprintf(fp, "Gerbicz checks = %" PRIu64 "\n", r.gerbicz_checks);
     std::fprintf(fp, "Gerbicz errors = %" PRIu64 "\n", r.gerbicz_errors);
   }
+  if (r.has_jacobi) {
+    std::fprintf(fp, "Jacobi checks = %" PRIu64 "\n", r.jacobi_checks);
+    std::fprintf(fp, "Jacobi errors = %" PRIu64 "\n", r.jacobi_errors);
+  }
   return std::fclose(fp) == 0;
 }
 

@@ -40,6 +40,8 @@ struct StatsRecord {
   uint64_t res64 = 0;
   bool has_gerbicz = false;
   uint64_t gerbicz_checks = 0, gerbicz_errors = 0;
+  bool has_jacobi = false;
+  uint64_t jacobi_checks = 0, jacobi_errors = 0;
 };
 
 // DumpStats (lucas_prp.cu:293-324): same keys, same order, same %g formats;

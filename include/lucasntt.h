@@ -78,7 +78,9 @@ int lnt_create(uint32_t exponent, uint32_t n, int prp, int device, lnt_test** ou
  * and kernels by timing PerformanceLoops iterations of each
  * (Process::GetBestPerformers, process.cu:45-127; KernelPool, kernel_pool.cu:17-142;
  * LucasPRP::LucasPRP, lucas_prp.cu:36-70).  Here a plan is the kernel family,
- * the 4-step split and the column tile of one NTT length. */
+ * the 4-step split, the column tile, the pass radix and the fusion depth of one
+ * NTT length (the reference's kernel choice, butterflies per thread and
+ * transpose tile, kernel.cu:157-192, :257-287). */
 typedef enum lnt_plan_kind {
   LNT_PLAN_AUTO = 0,     /* the policy's choice */
   LNT_PLAN_RESIDENT = 1, /* n <= 4096: one CTA per residue, state in shared memory (FFT_1SMEM) */
@@ -90,6 +92,10 @@ typedef struct lnt_plan_options {
   uint32_t kind;      /* lnt_plan_kind */
   uint32_t log2_rows; /* two-pass: log2 of the column length n2 (n = n2 x n1); 0 = policy */
   uint32_t tile;      /* two-pass: columns per column CTA = words per carry run, 4 or 8; 0 = policy */
+  uint32_t radix;     /* LNT_PLAN_RADIX16: largest pass radix, 8 or 16; 0 = policy (8) */
+  uint32_t fused;     /* LNT_PLAN_RADIX16: 1 = the inverse column pass of a squaring and the
+                         forward one of the next in one carry-fused launch, 2 = two launches;
+                         0 = policy (fused from 2^19 words) */
 } lnt_plan_options;
 
 /* lnt_create with an explicit plan (NULL = policy): the analogue of forcing
@@ -172,6 +178,39 @@ int lnt_gerbicz_enable(lnt_test* t, uint32_t block);
 /* Squarings verified so far (since enable / the last set_digits), checks
  * passed and errors detected (each followed by a rollback). */
 int lnt_gerbicz_stats(lnt_test* t, uint64_t* verified_iterations, uint64_t* checks, uint64_t* errors);
+
+/* ---- Jacobi error check (LL) ------------------------------------------------
+ * No counterpart in the reference (lucas_prp.cu:137-195 checks nothing).  For
+ * an LL sequence u_0 = 4, u_{k+1} = u_k^2 - 2, the Jacobi symbol
+ * (u_k - 2 | 2^q - 1) is -1 for every k >= 1; a residue whose symbol is not -1
+ * is wrong (an error leaves it at -1 about half of the time).  The symbol of a
+ * q-bit number needs GMP's subquadratic mpz_jacobi, loaded at run time from
+ * libgmp.so.10: LNT_ERR_UNSUPPORTED_LENGTH when it is not installed.  A host
+ * computation: seconds at q ~ 10^8, so checks belong at long intervals. */
+
+/* (s - 2 | 2^exponent - 1) for the residue s given by canonical digits (the
+ * dump order and widths of lnt_get_digits / lnt_get_widths): *symbol = -1, 0
+ * or +1.  No GPU needed. */
+int lnt_jacobi_of_digits(const uint64_t* digits, const uint8_t* widths, uint32_t n, uint32_t exponent,
+                         int* symbol);
+
+/* The symbol of a test's current residue (0 when the kernels flagged a carry
+ * outside the balanced-digit headroom).  Valid from the first squaring after
+ * lnt_init_test on: the start value 4 itself has symbol +1. */
+int lnt_jacobi_check(lnt_test* t, int* symbol);
+
+/* interval > 0: every `interval` squarings lnt_iterate checks the symbol; a
+ * residue with symbol -1 becomes the verified one, any other (or a carry flag)
+ * sends the test back to the last verified residue and the squarings since are
+ * redone; after 3 failures in a row without a pass it returns LNT_ERR_NUMERIC.
+ * Assumes the residue is an LL term u_k with k >= 1 at every check (tests
+ * started by lnt_init_test, or resumed from such a residue).  One residue-sized
+ * buffer.  interval = 0 turns it off; LNT_ERR_INVALID_ARGUMENT for PRP tests. */
+int lnt_jacobi_enable(lnt_test* t, uint64_t interval);
+
+/* Squarings verified, checks passed and errors detected (each followed by a
+ * rollback) since enable / the last set_digits. */
+int lnt_jacobi_stats(lnt_test* t, uint64_t* verified_iterations, uint64_t* checks, uint64_t* errors);
 
 /* Diagnostic without a reference counterpart, for tests of the check: adds 1
  * to word `word` of the device state, as a hardware error would corrupt it. */
@@ -286,23 +325,54 @@ int lnt_batch_autotune(lnt_batch* b, uint32_t loops);
  * 8 squarings of every group; 0: plain stream launches. */
 int lnt_batch_use_graphs(lnt_batch* b, int enable);
 
+/* Per-test Res64 checkpoints (no counterpart in the reference, which reports
+ * Res64 only at the end of a run, lucas_prp.cu:254-263, so its intermediate
+ * residues come from separate runs of k iterations): with every > 0 each test
+ * records the Res64 of its residue whenever its squaring count reaches a
+ * multiple of `every` below its target; 0 (default) turns this off.  Batched
+ * launches stop at the checkpoints, so they cost one readout per test each. */
+typedef struct lnt_batch_checkpoint {
+  uint64_t id;        /* as returned by lnt_batch_submit / lnt_batch_enqueue */
+  uint64_t iteration; /* squarings performed when the Res64 was taken */
+  uint64_t res64;
+  int status;         /* LNT_OK, or the readout's error */
+} lnt_batch_checkpoint;
+int lnt_batch_checkpoint_every(lnt_batch* b, uint64_t every);
+/* Move up to `cap` recorded checkpoints to `out` (count in *count). */
+int lnt_batch_poll_checkpoints(lnt_batch* b, lnt_batch_checkpoint* out, int cap, int* count);
+
+/* Autotuned plans cached in a JSON file (the analogue of the reference's
+ * per-run autotune summary, main_process.cu:160-190, kept across runs): plans
+ * in `path` measured on a GPU of this device's name are used instead of timing
+ * again, and every plan the batch tunes from now on is written back.  Takes
+ * effect with lnt_batch_autotune(b, loops > 0).  NULL turns the cache off. */
+int lnt_batch_plan_cache(lnt_batch* b, const char* path);
+
 /* No counterpart in the reference.  For callers that cannot allocate device
  * memory when they need a residue in the reference's digit format (a serving
  * process whose HBM is all handed to its own pool or budget, a latency-critical
  * step that must not pay cudaMalloc's implicit device synchronisation, a
- * checkpoint taken from an interrupt handler): turns n signed words `words`
- * (balanced or non-negative digits of a residue, widths `widths`) into the
- * reference's canonical digits, written to `digits`.  All three are DEVICE
- * pointers owned by the caller; nothing is allocated.  The scratch lives in one
- * library-owned array of device memory sized for n <= 2^24 (about 2.5 MiB, held
- * by every GPU that loads the library until exit); larger n is rejected with
- * LNT_ERR_INVALID_ARGUMENT.  prp / zero_start select the reference's
- * representation of 0 mod M (LL: 0; PRP: M unless the test started from zero).
- * The first call on a device sets up the scratch address, so make it before
- * any stream capture.  Every call shares the one array: calls that overlap on
- * the GPU (other streams, other threads) race.  Runs on `cuda_stream` (NULL =
- * legacy default stream) and returns after it finished (LNT_ERR_NUMERIC if
- * the words were too far from normalised digits). */
+ * checkpoint written by a path that must not allocate): turns n signed words
+ * `words` (widths `widths`) into the reference's canonical digits, written to
+ * `digits`.  The words must be the whole residue: any digits, balanced or
+ * non-negative, whose weighted sum is the value, with no carry pending
+ * elsewhere (lnt_get_raw_state of a RESIDENT-plan test qualifies; that of a
+ * two-pass test does not, since its run carries are held apart).  All three are
+ * DEVICE pointers owned by the caller; nothing is allocated.  The scratch lives
+ * in one library-owned array of device memory sized for n <= 2^24 (about
+ * 2.5 MiB, held by every GPU that loads the library until exit); larger n is
+ * rejected with LNT_ERR_INVALID_ARGUMENT.  prp / zero_start select the
+ * reference's representation of 0 mod M (LL: 0; PRP: M unless the test started
+ * from zero).  The first call on a device sets up the scratch address, so make
+ * it before any stream capture; a device reset invalidates that address (do not
+ * call this after cudaDeviceReset).  Every call shares the one array: calls
+ * that overlap on the GPU (other streams, other threads) race.  Runs on
+ * `cuda_stream` (NULL = legacy default stream; a stream must belong to the
+ * current device, else LNT_ERR_INVALID_ARGUMENT) and returns after it
+ * finished.  LNT_ERR_NUMERIC: the words were too far from normalised digits
+ * (a carry that does not settle within one block of 64 words); `digits` is
+ * then undefined, although lnt_get_digits of a test may still read such words
+ * (it falls back to an exact carry on the host). */
 int lnt_canonicalize_noalloc(const int64_t* words, const uint8_t* widths, uint32_t n, int prp,
                              int zero_start, uint64_t* digits, void* cuda_stream);
 

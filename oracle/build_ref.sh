@@ -6,8 +6,11 @@
 # binary on a B200 to pin residues and timings against the reference's own
 # build.  The reference needs `--pre-include cstdint` with this nvcc/gcc
 # (common/common.cuh uses uint32_t without including <cstdint>).
+#
+# Usage: oracle/build_ref.sh [REFERENCE_DIR]; the directory defaults to
+# $LNT_REFERENCE_DIR, else to where this build's reference checkout lives.
 set -euo pipefail
-REF=${1:-/root/reference}
+REF=${1:-${LNT_REFERENCE_DIR:-/root/reference}}
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
 if [ ! -d "$REF" ]; then

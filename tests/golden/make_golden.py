@@ -32,6 +32,7 @@ from pathlib import Path
 ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 
+from bench import c3_exponents, c4_exponents, c5_pool  # noqa: E402  (the workloads' seeded exponents)
 from oracle import bigint_model as B  # noqa: E402
 from oracle import oracle as O  # noqa: E402
 
@@ -39,47 +40,6 @@ HERE = Path(__file__).resolve().parent
 
 C1_EXPONENTS = [44497, 44501, 44507, 44519, 44531, 44533, 44537, 44543, 44549]
 C2_EXPONENT = 139000003
-
-
-def primes_between(lo: int, hi: int) -> list[int]:
-    import numpy as np
-
-    sieve = np.ones(hi + 1, dtype=bool)
-    sieve[:2] = False
-    for k in range(2, int(hi ** 0.5) + 1):
-        if sieve[k]:
-            sieve[k * k::k] = False
-    return [int(x) for x in np.nonzero(sieve)[0] if x >= lo]
-
-
-def c3_exponents() -> list[int]:
-    """256 primes in [1e5, 2e6], random.Random(0).sample (the C3 batch)."""
-    import random
-
-    return random.Random(0).sample(primes_between(100000, 2000000), 256)
-
-
-def c4_exponents() -> list[int]:
-    """64 primes in [5e6, 2e7], random.Random(1).sample (the C4 PRP batch)."""
-    import random
-
-    return random.Random(1).sample(primes_between(5000000, 20000000), 64)
-
-
-def c5_pool(lo: int = 10000, hi: int = 30000000, count: int = 64) -> list[tuple[int, bool]]:
-    """The serving stream's request pool: `count` draws of (q, prp), q the
-    smallest prime >= exp(U(ln lo, ln hi)), prp by a fair coin, random.Random(2)."""
-    import bisect
-    import math
-    import random
-
-    primes = primes_between(lo, hi + 100000)
-    rng = random.Random(2)
-    out = []
-    for _ in range(count):
-        x = math.exp(rng.uniform(math.log(lo), math.log(hi)))
-        out.append((primes[min(bisect.bisect_left(primes, int(x)), len(primes) - 1)], rng.random() < 0.5))
-    return out
 
 
 def is_prime(k: int) -> bool:

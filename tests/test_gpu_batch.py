@@ -80,3 +80,129 @@ def test_batch_budget_admission_and_refill(lnt):
         assert set(rest) == {a2, a3}
         assert rest[a3]["res64"] == alone(lnt, q + 66, 0, False, 5)
         assert b.status() == (0, 0)
+
+
+def _primes_from(lo, count):
+    out, k = [], lo
+    while len(out) < count:
+        if all(k % d for d in range(2, int(k ** 0.5) + 1)):
+            out.append(k)
+        k += 1
+    return out
+
+
+def test_fused_groups_beside_resident_tests(lnt):
+    """Two carry-fused groups (2^19 and 2^20 words, 44 tests each, on their own
+    streams) and 20 SMEM-resident tests running thousands of squarings in one
+    launch beside them, graphs on.  A fused CTA waits only for CTAs that started
+    before it, so however the other launches hold the GPU's CTA slots no wait
+    runs out (that would fail the batch with a timeout status) and every test
+    ends with the residue it gets alone."""
+    resident = _primes_from(60000, 20)
+    fused = _primes_from(8000000, 44) + _primes_from(12000000, 44)
+    assert {lnt.secured_log2_length(q) for q in fused[:44]} == {19}
+    assert {lnt.secured_log2_length(q) for q in fused[44:]} == {20}
+    k_res, k_fused = 6000, 17  # the two-pass tests: one squaring alone, then 2 graph chunks of 8
+    jobs = {}
+    with lnt.Batch(device=0, graphs=True) as b:
+        for i, q in enumerate(resident):
+            jobs[b.submit(q, 0, bool(i & 1), k_res)] = (q, bool(i & 1), k_res)
+        for i, q in enumerate(fused):
+            jobs[b.submit(q, 0, bool(i & 1), k_fused)] = (q, bool(i & 1), k_fused)
+        assert b.status()[0] == len(jobs)
+        got = {}
+        for _ in range(20):
+            b.run(3000)
+            for r in b.poll():
+                assert r["status"] == 0, r
+                got[r["id"]] = r
+            if len(got) == len(jobs):
+                break
+        assert b.status()[0] == 0
+    assert set(got) == set(jobs)
+    for i, (q, prp, k) in jobs.items():
+        assert got[i]["res64"] == alone(lnt, q, 0, prp, k), (q, prp, k)
+
+
+def test_batch_checkpoints_equal_alone(lnt):
+    """Res64 checkpoints every 100 squarings of a resident, a two-pass and a
+    carry-fused test (LL and PRP) equal the same test alone after 100, 200 and
+    300 squarings; the final result comes at 350."""
+    tests = [(44497, 0, False), (160001, 0, True), (8000009, 0, False)]
+    with lnt.Batch(device=0, checkpoint_every=100) as b:
+        ids = {b.submit(q, n, prp, 350): (q, n, prp) for q, n, prp in tests}
+        done, marks = {}, {}
+        while len(done) < len(ids):
+            b.run(64)
+            for c in b.poll_checkpoints():
+                assert c["status"] == 0, c
+                marks.setdefault(c["id"], {})[c["iteration"]] = c["res64"]
+            for r in b.poll():
+                done[r["id"]] = r
+    for i, (q, n, prp) in ids.items():
+        assert sorted(marks[i]) == [100, 200, 300], (q, marks.get(i))
+        with lnt.LucasTest(q, n, prp) as t:
+            for k in (100, 200, 300):
+                t.iterate(100)
+                assert t.res64() == marks[i][k], (q, k)
+            t.iterate(50)
+            assert t.res64() == done[i]["res64"]
+
+
+def test_batch_autotune_plan_cache(lnt, tmp_path):
+    """A tuned plan is written to the JSON cache and a later batch uses it
+    without timing again; the residues equal the policy plan's."""
+    import json
+
+    path = tmp_path / "plans.json"
+    q = 1000003
+    with lnt.Batch(device=0, autotune_loops=5, plan_cache=str(path)) as b:
+        i = b.submit(q, 0, False, 40)
+        b.run(40)
+        r1 = {r["id"]: r for r in b.poll()}[i]
+    cache = json.loads(path.read_text())
+    assert cache["plans"] and cache["plans"][0]["n"] == 65536
+    chosen = cache["plans"][0]
+    before = path.read_text()
+    with lnt.Batch(device=0, autotune_loops=5, plan_cache=str(path)) as b:
+        i = b.submit(q + 30, 0, False, 40)  # same length and carry-run class: the cached plan
+        b.run(40)
+        r2 = {r["id"]: r for r in b.poll()}[i]
+    assert path.read_text() == before
+    assert r1["res64"] == alone(lnt, q, 0, False, 40)
+    assert r2["res64"] == alone(lnt, q + 30, 0, False, 40)
+    assert chosen["radix"] in (8, 16) and chosen["fused"] in (1, 2)
+
+
+def test_serving_admits_requests_mid_flight(lnt):
+    """Continuous batching: requests enqueued while others are running, across
+    the resident (n <= 4096), two-pass and carry-fused (n >= 2^19) plans, LL and
+    PRP, under a budget that holds only part of them at once, so later requests
+    wait and are admitted as earlier ones retire.  Each result equals the same
+    test alone."""
+    first = [(44497, False, 3000), (160001, True, 400), (8000009, False, 60)]
+    later = [(9941, True, 2500), (300007, False, 300), (12000017, True, 40), (59063, False, 2000),
+             (1000003, True, 200)]
+    # the 2^20-word request cannot join the 2^19-word one: it waits for it to retire
+    budget = lnt.test_device_bytes(8000009) + lnt.test_device_bytes(12000017) - 1
+    jobs, got = {}, {}
+    with lnt.Batch(device=0, hbm_budget_bytes=budget) as b:
+        for q, prp, k in first:
+            jobs[b.enqueue(q, 0, prp, k)] = (q, prp, k)
+        b.run(25)  # the first requests are mid-flight
+        assert not b.poll()
+        for q, prp, k in later:
+            jobs[b.enqueue(q, 0, prp, k)] = (q, prp, k)
+        waited = b.pending() > 0
+        for _ in range(500):
+            b.run(100)
+            for r in b.poll():
+                assert r["status"] == 0, r
+                got[r["id"]] = r
+            if len(got) == len(jobs):
+                break
+        assert b.status()[0] == 0 and b.pending() == 0
+    assert waited, "the budget should have held some requests back"
+    assert set(got) == set(jobs)
+    for i, (q, prp, k) in jobs.items():
+        assert got[i]["res64"] == alone(lnt, q, 0, prp, k), (q, prp, k)

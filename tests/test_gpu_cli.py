@@ -90,13 +90,17 @@ def test_composite_verdict(tmp_path):
     assert stats(tmp_path / "c.txt")["Conclusion"] == "Composite"
 
 
-@pytest.mark.parametrize("case", [c for c in REF if c["n"] <= 4096], ids=lambda c: f"{c['q']}@{c['n']}")
+@pytest.mark.parametrize("case", [c for c in REF if c["n"] <= 4096],
+                         ids=lambda c: f"{c['q']}@{c['n']}{'_prp' if c['prp'] else ''}")
 def test_dump_file_equals_reference_c1(tmp_path, case):
-    """Full LL with dumpResidue = 1: the .dat file is the reference's, byte for byte."""
+    """Full LL and PRP tests with dumpResidue = 1 (the C1 exponents, the
+    serving stream's small exponents, PRP fulls): the .dat file is the
+    reference's, byte for byte."""
     args = [case["q"], case["iterations"], "run"]
-    if case["n"] != 1 << (2047).bit_length():  # the forced length 4096 needs the fft argument
-        args.append(case["n"])
-    r = run_cli(tmp_path, args, ini="dumpResidue = 1\nPerformanceLoops = 100\n", stdin="Y\n")
+    if case["q"] in (44497, 44501, 44507, 44519, 44531, 44533, 44537, 44543, 44549) and case["n"] == 4096:
+        args.append(case["n"])  # the forced length 4096 needs the fft argument
+    prp = "PRP = 1\n" if case["prp"] else ""
+    r = run_cli(tmp_path, args, ini=prp + "dumpResidue = 1\nPerformanceLoops = 100\n", stdin="Y\n")
     assert r.returncode == 0, r.stdout + r.stderr
     s = stats(tmp_path / "run.txt")
     assert s["n"] == str(case["n"])
@@ -104,10 +108,13 @@ def test_dump_file_equals_reference_c1(tmp_path, case):
     assert sha256(tmp_path / "run.dat") == case["dump_sha256"]
 
 
-@pytest.mark.parametrize("case", [c for c in REF if c["n"] == 1 << 23], ids=lambda c: str(c["iterations"]))
+@pytest.mark.parametrize("case", [c for c in REF if c["n"] == 1 << 23],
+                         ids=lambda c: f"{c['iterations']}{'_prp' if c['prp'] else ''}")
 def test_dump_file_equals_reference_c2(tmp_path, case):
-    """q = 139000003 at 2^23: a partial run always dumps (lucas_prp.cu:189); same bytes."""
-    r = run_cli(tmp_path, [case["q"], case["iterations"], "c2"], ini="PerformanceLoops = 100\n")
+    """q = 139000003 at 2^23, LL and PRP: a partial run always dumps
+    (lucas_prp.cu:189); same bytes."""
+    prp = "PRP = 1\n" if case["prp"] else ""
+    r = run_cli(tmp_path, [case["q"], case["iterations"], "c2"], ini=prp + "PerformanceLoops = 100\n")
     assert r.returncode == 0, r.stdout + r.stderr
     assert f"{case['iterations']} loops performed with M({case['q']})" in r.stdout
     s = stats(tmp_path / "c2.txt")
@@ -199,3 +206,12 @@ def test_pool_preference(tmp_path, lnt):
     r = run_cli(tmp_path, [1000003, 200, "p"], ini=f"PerformanceLoops = 50\nPool = {name}\n")
     assert r.returncode == 0, r.stdout
     assert stats(tmp_path / "p.txt")["Pool"] == name
+
+
+def test_jacobi_check_from_the_ini(tmp_path):
+    """JacobiCheck (an extension key): a checked LL test of M_132049, checks in the stats file."""
+    r = run_cli(tmp_path, [132049, 0, "j"], ini="PerformanceLoops = 50\nJacobiCheck = 20000\n")
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "M(132049) is prime!" in r.stdout
+    s = stats(tmp_path / "j.txt")
+    assert s["Jacobi checks"] == str((132049 - 2) // 20000) and s["Jacobi errors"] == "0"

@@ -84,3 +84,43 @@ def test_carry_flag_from_a_corrupted_word_is_recovered(lnt, at):
         assert st["errors"] >= 1
         assert st["checks"] == iterations // (block * block)
         assert t.res64() == plain_res64(lnt, q, iterations)
+
+
+def test_jacobi_check_ll(lnt):
+    """LL error check: the symbol of an LL residue is -1 after every checked
+    interval, a full test of M_132049 passes every check, and a word corrupted
+    between calls is detected (now or, since an error leaves the symbol at -1
+    half of the time, at a later check after more corruptions) and rolled
+    back: the final residue equals the unchecked one."""
+    import ctypes
+
+    L = lnt.lib()
+    with lnt.LucasTest(132049, 0, False) as T:
+        L.lnt_jacobi_enable.argtypes = [ctypes.c_void_p, ctypes.c_uint64]
+        assert L.lnt_jacobi_enable(T._h, 5000) == 0, L.lnt_last_error()
+        T.iterate(132049 - 2)
+        assert T.is_prime()
+        v, c, e = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        assert L.lnt_jacobi_stats(T._h, ctypes.byref(v), ctypes.byref(c), ctypes.byref(e)) == 0
+        assert c.value == (132049 - 2) // 5000 and e.value == 0
+    q = 1000003
+    with lnt.LucasTest(q, 0, False) as ref:
+        ref.iterate(400)
+        want = ref.res64()
+    caught = 0
+    for k in range(20):  # a changed word leaves the symbol at -1 half of the time: try words until one is caught
+        with lnt.LucasTest(q, 0, False) as T:
+            assert L.lnt_jacobi_enable(T._h, 100) == 0
+            T.iterate(100)
+            s = ctypes.c_int()
+            assert L.lnt_jacobi_check(T._h, ctypes.byref(s)) == 0 and s.value == -1
+            T.debug_corrupt(word=17 + 31 * k, delta=1)
+            T.iterate(300)
+            v, c, e = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+            assert L.lnt_jacobi_stats(T._h, ctypes.byref(v), ctypes.byref(c), ctypes.byref(e)) == 0
+            if e.value:
+                assert e.value == 1 and v.value == 400
+                assert T.res64() == want  # rolled back and redone
+                caught += 1
+                break
+    assert caught == 1

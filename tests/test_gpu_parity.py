@@ -149,25 +149,65 @@ def test_two_pass_known_prime(lnt):
         assert T.is_prime()
 
 
+def _reference_cases():
+    return json.loads((GOLDEN / "ref_residues.json").read_text())["cases"]
+
+
 def test_reference_build_residues(lnt):
-    """Res64 equal to the reference's own build (run on a B200): C1 full
-    tests at n = 2048 and 4096, and q = 139000003 after 1000 and 10000
-    squarings at n = 2^23."""
-    cases = json.loads((GOLDEN / "ref_residues.json").read_text())["cases"]
-    c2 = sorted((c for c in cases if c["q"] == 139000003), key=lambda c: c["iterations"])
+    """Res64 equal to the reference's own build (run on a B200), each test
+    alone: C1 full LL tests at n = 2048 and 4096; q = 139000003 after 1,000 and
+    10,000 LL squarings and 1,000 PRP squarings at n = 2^23; full PRP tests of
+    Mersenne primes (residue 9) and composites on the resident and two-pass
+    plans; one C4 exponent per length (PRP, 20,000 squarings); the C3 full LL
+    tests up to 32K words."""
+    cases = _reference_cases()
+    c2 = sorted((c for c in cases if c["q"] == 139000003 and not c["prp"]), key=lambda c: c["iterations"])
+    c4_lengths = {}
     for c in cases:
-        if c["q"] == 139000003:
-            continue
+        if c.get("set") == "c4":
+            c4_lengths.setdefault(c["n"], c)
+    alone_cases = [c for c in cases if c.get("set") in (None, "prp") and c not in c2]
+    alone_cases += list(c4_lengths.values())
+    alone_cases += [c for c in cases if c.get("set") == "c3_full" and c["n"] <= 32768]
+    assert len(c4_lengths) == 3 and sum(c["prp"] for c in alone_cases) >= 9
+    for c in alone_cases:
         with lnt.LucasTest(c["q"], c["n"], c["prp"]) as T:
             T.iterate(c["iterations"])
             assert f"{T.res64():016x}" == c["res64"], c
-            assert T.is_prime() == (c["conclusion"] == "Prime")
+            assert T.is_prime() == (c["conclusion"] in ("Prime", "Probably Prime")), c
     with lnt.LucasTest(139000003, 1 << 23, False) as T:
         done = 0
         for c in c2:
             T.iterate(c["iterations"] - done)
             done = c["iterations"]
             assert f"{T.res64():016x}" == c["res64"], c
+
+
+def test_reference_build_residues_in_one_batch(lnt):
+    """Every pinned reference-build residue at once in one batch: resident,
+    two-pass and carry-fused plans, LL and PRP mixed -- the nine C1 tests, the
+    64 C4 PRP tests (20,000 squarings), the 256 C3 exponents (20,000 LL
+    squarings) and one full C3 test per length, the serving stream's full tests
+    up to q = 610,000, the PRP full tests and the C2 exponent (1,000 squarings
+    LL and PRP).  Each Res64 equals the reference build's."""
+    cases = [c for c in _reference_cases() if not (c["q"] == 139000003 and c["iterations"] == 10000)]
+    want = {}
+    with lnt.Batch(device=0) as b:
+        for c in cases:
+            i = b.submit(c["q"], c["n"], c["prp"], c["iterations"])
+            want[i] = c
+        got = {}
+        for _ in range(2000):
+            b.run(4000)
+            for r in b.poll():
+                got[r["id"]] = r
+            if len(got) == len(want):
+                break
+        assert b.status()[0] == 0
+    assert set(got) == set(want)
+    bad = [(want[i]["q"], want[i]["n"], want[i]["prp"], want[i]["iterations"])
+           for i, r in got.items() if r["status"] != 0 or f"{r['res64']:016x}" != want[i]["res64"]]
+    assert not bad, bad[:10]
 
 
 def test_device_arithmetic_against_host(lnt):

@@ -148,3 +148,4 @@ def test_oracle_matches_reference_build_prp_and_batch_pins(oracle_mod):
         with oracle_mod.OracleTest(c["q"], c["n"], c["prp"]) as T:
             T.iterate(c["iterations"])
             assert f"{T.res64():016x}" == c["res64"], c
+

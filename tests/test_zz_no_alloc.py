@@ -3,12 +3,13 @@
 Some callers cannot allocate device memory when they need a residue in the
 reference's digit format: a serving process that has handed all of its HBM to
 its own pool or admission budget, a latency-critical step that must not pay
-cudaMalloc's implicit device synchronisation, a checkpoint written from an
-interrupt handler.  They pass their own device buffers to
+cudaMalloc's implicit device synchronisation, a checkpoint written by a path
+that must not allocate.  They pass their own device buffers to
 lnt_canonicalize_noalloc, whose scratch is one fixed library-owned array
 (residues up to 2^24 words).  Its digits must equal the regular readout's
 exactly (integer digits: the tolerance is zero), on two calls in a row that
-share that array.
+share that array; up to the 2^24 limit they must equal canonical digits that
+the test chose itself, rebuilt from perturbed balanced words.
 
 This file is named to be collected last.
 """
@@ -82,3 +83,62 @@ def test_noalloc_rejects_sizes_beyond_its_scratch(lnt):
         assert fn(dummy.data_ptr(), dummy.data_ptr(), n, 0, 0, dummy.data_ptr(), None) == 1
     assert fn(None, dummy.data_ptr(), 8, 0, 0, dummy.data_ptr(), None) == 1
     assert b"2^24" in lnt.lib().lnt_last_error() or b"null" in lnt.lib().lnt_last_error()
+
+
+def _balanced_words(rng, widths):
+    """Random canonical digits d (value below M, not all maximal) and signed
+    words of the same value: each digit above half its range borrows 2^w from
+    the next word (cyclically: 2^q = 1 mod M), then random multiples of 2^w move
+    between neighbours."""
+    w = widths.astype(np.int64)
+    d = (rng.integers(0, 1 << 62, size=w.size, dtype=np.int64) & ((np.int64(1) << w) - 1))
+    d[-1] = 0  # not all maximal
+    c = (d >= (np.int64(1) << (w - 1))).astype(np.int64)
+    b = d - (c << w) + np.roll(c, 1)
+    k = rng.integers(-3, 4, size=w.size, dtype=np.int64)
+    b = b - (k << w) + np.roll(k, 1)
+    return d.astype(np.uint64), b
+
+
+@pytest.mark.parametrize("q,log2n", [(1000003, 16), (20000003, 20), (300000007, 24)])
+def test_noalloc_at_size_limit(lnt, q, log2n):
+    """n = 2^16, 2^20 and the declared limit 2^24 (262,144 scan blocks, the
+    whole scratch array): two calls in a row, each digit equal to the
+    canonical digits the words were built from."""
+    import torch
+
+    n = 1 << log2n
+    assert lnt.secured_log2_length(q) == log2n
+    dev = torch.device("cuda", 0)
+    fn = _noalloc()
+    with lnt.LucasTest(q, n, False) as T:
+        widths_host = T.widths()
+    widths = torch.from_numpy(widths_host).to(dev)
+    out = torch.empty(n, dtype=torch.int64, device=dev)
+    rng = np.random.default_rng(q)
+    for _ in range(2):
+        want, words_host = _balanced_words(rng, widths_host)
+        words = torch.from_numpy(words_host).to(dev)
+        out.fill_(-1)
+        stream = torch.cuda.current_stream(dev)
+        status = fn(words.data_ptr(), widths.data_ptr(), n, 0, 0, out.data_ptr(), stream.cuda_stream)
+        assert status == 0, lnt.lib().lnt_last_error()
+        got = out.cpu().numpy().view(np.uint64)
+        bad = np.nonzero(got != want)[0]
+        assert bad.size == 0, (bad[:5], got[bad[:5]], want[bad[:5]])
+
+
+def test_noalloc_reports_words_far_from_normalised(lnt):
+    """Words whose carries do not settle within a block (here 2^40 over eight
+    1-bit digits) return LNT_ERR_NUMERIC with the reason, not wrong digits."""
+    import torch
+
+    dev = torch.device("cuda", 0)
+    fn = _noalloc()
+    words = torch.full((8,), 1 << 40, dtype=torch.int64, device=dev)
+    widths = torch.ones(8, dtype=torch.uint8, device=dev)
+    out = torch.empty(8, dtype=torch.int64, device=dev)
+    status = fn(words.data_ptr(), widths.data_ptr(), 8, 0, 0, out.data_ptr(),
+                torch.cuda.current_stream(dev).cuda_stream)
+    assert status == 5, status  # LNT_ERR_NUMERIC
+    assert b"too far from normalised" in lnt.lib().lnt_last_error()
