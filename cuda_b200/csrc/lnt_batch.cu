@@ -57,13 +57,17 @@ struct Pending {
   Clock::time_point enqueued;
 };
 
-// Tests share launches when their kernels see the same geometry.
+// Tests share launches when their kernels see the same geometry: length,
+// split, tile, pass radix (the pass tables differ) and column fusion.
 struct GroupKey {
-  uint32_t n, log2n2, tile;
+  uint32_t n, log2n2, tile, radix;
+  bool fused;
   bool operator<(const GroupKey& o) const {
     if (n != o.n) return n < o.n;
     if (log2n2 != o.log2n2) return log2n2 < o.log2n2;
-    return tile < o.tile;
+    if (tile != o.tile) return tile < o.tile;
+    if (radix != o.radix) return radix < o.radix;
+    return fused < o.fused;
   }
 };
 
@@ -220,8 +224,8 @@ int rebuild(lnt_batch* b) {
     if (p.kind == lnt::PlanKind::Resident) {
       b->resident.push_back(i);
     } else if (p.fast && lnt::test_ready_for_group(b->active[i].t)) {
-      // one launch serves tests of identical geometry: same length and tile width
-      Group& g = b->groups[GroupKey{p.n, p.log2n2, p.tile}];
+      // one launch serves tests of identical geometry
+      Group& g = b->groups[GroupKey{p.n, p.log2n2, p.tile, p.radix, p.fused}];
       g.n = p.n;
       g.fused = p.fused;
       g.members.push_back(i);

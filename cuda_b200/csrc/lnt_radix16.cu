@@ -32,6 +32,11 @@ constexpr int row_threads_for(int L) { return L <= 4096 ? 256 : (L == 8192 ? 512
 #ifndef LNT_ROW_MIN_BLOCKS
 #define LNT_ROW_MIN_BLOCKS 4  // CTAs per SM the row kernel is compiled for (registers)
 #endif
+// Radix-16 passes hold 16 values and their twiddles per thread: at the 64
+// registers of four row CTAs (two 4-column CTAs) per SM they spill, so their
+// kernels are built for half the CTAs per SM (128 registers, no spills).
+template <int TH, int MR>
+constexpr int row_min_blocks() { return TH == 256 ? (MR == 16 ? 2 : LNT_ROW_MIN_BLOCKS) : 1024 / TH; }
 
 // Forward pass of `rows` row transforms.  The first pass (span = L) reads HBM
 // and applies the 4-step twiddle; later passes read shared memory.  One code
@@ -139,7 +144,7 @@ __device__ __forceinline__ void row_pass_r(int R, uint64_t* sm, int ld, int rows
 }
 
 template <int TH, int MR>
-__global__ void __launch_bounds__(TH, TH == 256 ? LNT_ROW_MIN_BLOCKS : 1024 / TH) row_square_r16(const TwoPassDesc* __restrict__ Ds, Passes P, int rows) {
+__global__ void __launch_bounds__(TH, row_min_blocks<TH, MR>()) row_square_r16(const TwoPassDesc* __restrict__ Ds, Passes P, int rows) {
   extern __shared__ __align__(16) uint64_t sm[];
   const TwoPassDesc& D = Ds[blockIdx.y];
   const int L = (int)D.n1, ld = padded(L);
@@ -221,8 +226,8 @@ constexpr int col_threads() { return 128 * T; }
 #ifndef LNT_COL_MIN_BLOCKS
 #define LNT_COL_MIN_BLOCKS 2  // CTAs per SM the 4-column kernels are compiled for (registers)
 #endif
-template <int T>
-constexpr int col_min_blocks() { return T == 4 ? LNT_COL_MIN_BLOCKS : 1; }
+template <int T, int MR = 8>
+constexpr int col_min_blocks() { return T == 4 && MR == 8 ? LNT_COL_MIN_BLOCKS : 1; }
 
 // column stride in words: the coalesced staging (lanes = T columns x 32/T
 // rows) then hits distinct banks
@@ -322,6 +327,11 @@ __device__ __forceinline__ void load_widths(const uint8_t* src, unsigned (&out)[
 // Carry-in from the run before each row's run, weight, forward column passes,
 // store.  The tile's digits are in `sm`.  `cg_carries`: read the carries from L2
 // (written by another CTA of the same launch).
+// Column passes synchronise per column (named barriers) instead of per block.
+#ifndef LNT_COL_GROUP_SYNC
+#define LNT_COL_GROUP_SYNC 1
+#endif
+
 template <int T, int MR>
 __device__ __forceinline__ void forward_tile(const TwoPassDesc& D, const Passes& P, uint64_t* sm,
                                              int ld, uint32_t t0, bool apply_carries, bool cg_carries,
@@ -360,10 +370,18 @@ __device__ __forceinline__ void forward_tile(const TwoPassDesc& D, const Passes&
   __syncthreads();
   int span = L;
   for (int j = 0, seg = 0; j < P.m; ++j) {
+#if LNT_COL_GROUP_SYNC
+    // each column's passes touch only that column: its own threads' barrier,
+    // the block's before the tile leaves shared memory
+    pass_r_grouped<0, MR>(P.radix[j], sm, ld, T, L, span, D.itw2 + seg);
+    if (j + 1 < P.m) group_sync(T);
+    else __syncthreads();
+#else
     pass_r<0, MR>(P.radix[j], sm, ld, T, L, span, D.itw2 + seg);
+    __syncthreads();
+#endif
     seg += span;
     span /= P.radix[j];
-    __syncthreads();
   }
   tile_store(sm, ld, D.x, L, T, D.n1, t0 * T);
 }
@@ -378,8 +396,14 @@ __device__ __forceinline__ void inverse_tile(const TwoPassDesc& D, const Passes&
   int span = 1;
   for (int j = P.m - 1; j >= 0; --j) {
     span *= P.radix[j];
+#if LNT_COL_GROUP_SYNC
+    pass_r_grouped<1, MR>(P.radix[j], sm, ld, T, L, span, D.iitw2 + pass_table_offset(P, L, j));
+    if (j > 0) group_sync(T);
+    else __syncthreads();  // the carry step reads every column of a row
+#else
     pass_r<1, MR>(P.radix[j], sm, ld, T, L, span, D.iitw2 + pass_table_offset(P, L, j));
     __syncthreads();
+#endif
   }
   for (int r = threadIdx.x; r < L; r += blockDim.x) {
     const size_t run = (size_t)t0 * L + r;
@@ -399,7 +423,7 @@ __device__ __forceinline__ void inverse_tile(const TwoPassDesc& D, const Passes&
 }
 
 template <int T, int TH, int MR>
-__global__ void __launch_bounds__(TH, TH == col_threads<T>() ? col_min_blocks<T>() : 1) col_forward_r16(
+__global__ void __launch_bounds__(TH, TH == col_threads<T>() ? col_min_blocks<T, MR>() : 1) col_forward_r16(
     const TwoPassDesc* __restrict__ Ds, Passes P, int apply_carries) {
   extern __shared__ __align__(16) uint64_t sm[];
   const TwoPassDesc& D = Ds[blockIdx.y];
@@ -412,7 +436,7 @@ __global__ void __launch_bounds__(TH, TH == col_threads<T>() ? col_min_blocks<T>
 }
 
 template <int T, int TH, int MR>
-__global__ void __launch_bounds__(TH, TH == col_threads<T>() ? col_min_blocks<T>() : 1) col_inverse_r16(
+__global__ void __launch_bounds__(TH, TH == col_threads<T>() ? col_min_blocks<T, MR>() : 1) col_inverse_r16(
     const TwoPassDesc* __restrict__ Ds, Passes P, int unsigned_mode) {
   extern __shared__ __align__(16) uint64_t sm[];
   const TwoPassDesc& D = Ds[blockIdx.y];
@@ -483,7 +507,7 @@ __device__ __forceinline__ void wait_flag(const uint32_t* flag, uint32_t want, u
 }
 
 template <int T, int TH, int MR>
-__global__ void __launch_bounds__(TH, TH == col_threads<T>() ? col_min_blocks<T>() : 1) col_fused_r16(
+__global__ void __launch_bounds__(TH, TH == col_threads<T>() ? col_min_blocks<T, MR>() : 1) col_fused_r16(
     const TwoPassDesc* __restrict__ Ds, Passes P) {
   extern __shared__ __align__(16) uint64_t sm[];
   __shared__ uint32_t s_ticket, s_epoch;
@@ -506,38 +530,36 @@ __global__ void __launch_bounds__(TH, TH == col_threads<T>() ? col_min_blocks<T>
     return;
   }
   uint32_t status = 0;
+  const bool is_last = ticket == last;
 
-  if (ticket == last) {
+  // first halves, each inverse_tile / forward_tile body instantiated once (the
+  // kernel stays small for the instruction cache): ticket 0 does the last
+  // tile's and then tile 0's, ticket t < T-1 its own, ticket T-1 none
+  const int ninv = is_last ? 0 : (ticket == 0 ? 2 : 1);
+  for (int i = 0; i < ninv; ++i) {
+    const bool lasttile = ticket == 0 && i == 0;
+    const uint32_t tile = lasttile ? last : ticket;
+    tile_load(sm, ld, D.x, L, T, n1, tile * T);
+    __syncthreads();
+    inverse_tile<T, MR>(D, P, sm, ld, tile, false);
+    // the last tile's digits wait in x for the last ticket
+    if (lasttile) tile_store(sm, ld, D.x, L, T, n1, last * T);
+    publish_flag(ctl + 2 + tile, ready);
+  }
+  if (is_last) {
     // the last tile's first half was done by ticket 0 (digits in x)
     wait_flag(ctl + 2 + last, ready, D.status);
     tile_load_cg(sm, ld, D.x, L, T, n1, last * T);
-    wait_flag(ctl + 2 + last - 1, ready, D.status);
-    forward_tile<T, MR>(D, P, sm, ld, last, true, true, status);
-    if (threadIdx.x == 0) {
-      // every ticket of this launch is taken and every CTA has read the epoch
-      ctl[0] = 0;
-      __threadfence();
-      asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(ctl + 1), "r"(ready) : "memory");
-    }
-  } else {
-    if (ticket == 0) {
-      // first half of the last tile: its carries feed tile 0 below, its
-      // digits wait in x for the last ticket
-      tile_load(sm, ld, D.x, L, T, n1, last * T);
-      __syncthreads();
-      inverse_tile<T, MR>(D, P, sm, ld, last, false);
-      tile_store(sm, ld, D.x, L, T, n1, last * T);
-      publish_flag(ctl + 2 + last, ready);
-    }
-    // first half: inverse column transform of the tile, carries out
-    tile_load(sm, ld, D.x, L, T, n1, ticket * T);
-    __syncthreads();
-    inverse_tile<T, MR>(D, P, sm, ld, ticket, false);
-    publish_flag(ctl + 2 + ticket, ready);
-    // second half: carries in from the tile before (tile 0: the last tile,
-    // made by this CTA), weight, forward column transform
-    if (ticket > 0) wait_flag(ctl + 2 + ticket - 1, ready, D.status);
-    forward_tile<T, MR>(D, P, sm, ld, ticket, true, true, status);
+  }
+  // second half: carries in from the tile before (tile 0: the last tile, made
+  // by this CTA), weight, forward column transform
+  if (ticket > 0) wait_flag(ctl + 2 + ticket - 1, ready, D.status);
+  forward_tile<T, MR>(D, P, sm, ld, ticket, true, true, status);
+  if (is_last && threadIdx.x == 0) {
+    // every ticket of this launch is taken and every CTA has read the epoch
+    ctl[0] = 0;
+    __threadfence();
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(ctl + 1), "r"(ready) : "memory");
   }
   if (status) atomicOr(D.status, status);
 }

@@ -206,3 +206,28 @@ def test_serving_admits_requests_mid_flight(lnt):
     assert set(got) == set(jobs)
     for i, (q, prp, k) in jobs.items():
         assert got[i]["res64"] == alone(lnt, q, 0, prp, k), (q, prp, k)
+
+
+def test_batch_keeps_plans_of_one_length_apart(lnt, tmp_path):
+    """Tests of one length whose plans differ only in pass radix and column
+    fusion (here from a plan cache: carry-run class 4 -> radix 16, fused;
+    class 8 -> radix 8, two launches; both with 8-word tiles) run in separate
+    launch groups, since their pass tables differ: every residue equals the
+    test alone."""
+    import json
+
+    import torch
+
+    cache = tmp_path / "plans.json"
+    cache.write_text(json.dumps({"device": torch.cuda.get_device_name(0), "plans": [
+        {"n": 524288, "run": 4, "kind": 2, "log2_rows": 9, "tile": 8, "radix": 16, "fused": 1, "ms": 1},
+        {"n": 524288, "run": 8, "kind": 2, "log2_rows": 9, "tile": 8, "radix": 8, "fused": 2, "ms": 1}]}))
+    tests = [(6291587, False), (6291599, True), (5767789, False), (5767841, True)]
+    with lnt.Batch(device=0, autotune_loops=5, plan_cache=str(cache)) as b:
+        ids = {b.submit(q, 0, prp, 30): (q, prp) for q, prp in tests}
+        got = {}
+        while len(got) < len(ids):
+            b.run(30)
+            got.update({r["id"]: r for r in b.poll()})
+    for i, (q, prp) in ids.items():
+        assert got[i]["status"] == 0 and got[i]["res64"] == alone(lnt, q, 0, prp, 30), (q, prp)
