@@ -121,6 +121,7 @@ def lib() -> ctypes.CDLL:
         "lnt_debug_corrupt_add": ([vp, u32, ctypes.c_int64], i32),
         "lnt_batch_use_graphs": ([vp, i32], i32),
         "lnt_batch_checkpoint_every": ([vp, u64], i32),
+        "lnt_batch_autotune_group": ([vp, u32], i32),
         "lnt_batch_poll_checkpoints": ([vp, ctypes.POINTER(BatchCheckpoint), i32, ctypes.POINTER(i32)], i32),
         "lnt_batch_plan_cache": ([vp, cp], i32),
         "lnt_arith_selftest": ([i32, ctypes.POINTER(u64), ctypes.POINTER(u64)], i32),
@@ -325,7 +326,8 @@ class Batch:
     as they finish (lnt_batch_*)."""
 
     def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, autotune_loops: int = 0,
-                 graphs: bool = True, checkpoint_every: int = 0, plan_cache: str | None = None):
+                 graphs: bool = True, checkpoint_every: int = 0, plan_cache: str | None = None,
+                 autotune_group: int = 1):
         h = ctypes.c_void_p()
         _check(lib().lnt_batch_create(device, int(hbm_budget_bytes), ctypes.byref(h)), "lnt_batch_create")
         self._h = h
@@ -333,6 +335,8 @@ class Batch:
             _check(lib().lnt_batch_plan_cache(self._h, str(plan_cache).encode()), "lnt_batch_plan_cache")
         if autotune_loops:
             _check(lib().lnt_batch_autotune(self._h, int(autotune_loops)), "lnt_batch_autotune")
+        if autotune_group > 1:
+            _check(lib().lnt_batch_autotune_group(self._h, int(autotune_group)), "lnt_batch_autotune_group")
         if checkpoint_every:
             _check(lib().lnt_batch_checkpoint_every(self._h, int(checkpoint_every)), "lnt_batch_checkpoint_every")
         if not graphs:

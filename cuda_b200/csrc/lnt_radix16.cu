@@ -10,6 +10,7 @@
 // and the last inverse pass writes HBM directly; the last forward pass, the
 // pointwise square and the first inverse pass run in registers back to back.
 #include <map>
+#include <type_traits>
 #include <mutex>
 #include <utility>
 
@@ -29,6 +30,13 @@ using namespace smem;
 // 256 threads per row of up to 4096 words (four CTAs per SM); longer rows hold
 // one or two CTAs per SM, so their CTAs are wider to keep 32 warps per SM.
 constexpr int row_threads_for(int L) { return L <= 4096 ? 256 : (L == 8192 ? 512 : 1024); }
+// The squaring kernel's CTA for `rows` rows of L words: up to 4096 words take
+// two radix-8 tasks per thread per pass (256 threads for 4096 words, down to
+// one warp), longer rows as row_threads_for.
+constexpr int row_square_threads(int L, int rows) {
+  return L > 4096 ? row_threads_for(L)
+                  : (L * rows >= 4096 ? 256 : (L * rows >= 2048 ? 128 : (L * rows >= 1024 ? 64 : 32)));
+}
 #ifndef LNT_ROW_MIN_BLOCKS
 #define LNT_ROW_MIN_BLOCKS 4  // CTAs per SM the row kernel is compiled for (registers)
 #endif
@@ -36,7 +44,10 @@ constexpr int row_threads_for(int L) { return L <= 4096 ? 256 : (L == 8192 ? 512
 // registers of four row CTAs (two 4-column CTAs) per SM they spill, so their
 // kernels are built for half the CTAs per SM (128 registers, no spills).
 template <int TH, int MR>
-constexpr int row_min_blocks() { return TH == 256 ? (MR == 16 ? 2 : LNT_ROW_MIN_BLOCKS) : 1024 / TH; }
+constexpr int row_min_blocks() {
+  return TH == 256 ? (MR == 16 ? 2 : LNT_ROW_MIN_BLOCKS)
+                   : ((MR == 16 ? 512 : 1024) / TH > 0 ? (MR == 16 ? 512 : 1024) / TH : 1);
+}
 
 // Forward pass of `rows` row transforms.  The first pass (span = L) reads HBM
 // and applies the 4-step twiddle; later passes read shared memory.  One code
@@ -220,14 +231,17 @@ __global__ void __launch_bounds__(TH) row_mul_r16(const TwoPassDesc* __restrict_
 
 // --------------------------------------------------------------- columns ----
 
-// column CTAs: 128 threads per tile column (T = 8: 1024 threads, T = 4: 512)
-template <int T>
-constexpr int col_threads() { return 128 * T; }
-#ifndef LNT_COL_MIN_BLOCKS
-#define LNT_COL_MIN_BLOCKS 2  // CTAs per SM the 4-column kernels are compiled for (registers)
-#endif
-template <int T, int MR = 8>
-constexpr int col_min_blocks() { return T == 4 && MR == 8 ? LNT_COL_MIN_BLOCKS : 1; }
+// Threads per tile column: one per radix-8 task of a pass (n2 / 8), at least a
+// warp and at most 128, or 256 for columns of 4096 words (one 4-column CTA per
+// SM).  Short columns (small lengths) thus get small CTAs, many per SM, instead
+// of CTAs whose threads mostly idle.
+__host__ __device__ constexpr int col_tpc(uint32_t n2) {
+  return n2 >= 4096 ? 256 : (n2 >= 1024 ? 128 : (n2 == 512 ? 64 : 32));
+}
+// CTAs per SM the column kernels are compiled for: 64 registers a thread at
+// 1024 threads an SM (128 for radix-16 passes, which spill at 64)
+template <int TH, int MR>
+constexpr int col_min_blocks() { return (MR == 16 ? 512 : 1024) / TH > 0 ? (MR == 16 ? 512 : 1024) / TH : 1; }
 
 // column stride in words: the coalesced staging (lanes = T columns x 32/T
 // rows) then hits distinct banks
@@ -327,11 +341,6 @@ __device__ __forceinline__ void load_widths(const uint8_t* src, unsigned (&out)[
 // Carry-in from the run before each row's run, weight, forward column passes,
 // store.  The tile's digits are in `sm`.  `cg_carries`: read the carries from L2
 // (written by another CTA of the same launch).
-// Column passes synchronise per column (named barriers) instead of per block.
-#ifndef LNT_COL_GROUP_SYNC
-#define LNT_COL_GROUP_SYNC 1
-#endif
-
 template <int T, int MR>
 __device__ __forceinline__ void forward_tile(const TwoPassDesc& D, const Passes& P, uint64_t* sm,
                                              int ld, uint32_t t0, bool apply_carries, bool cg_carries,
@@ -370,16 +379,8 @@ __device__ __forceinline__ void forward_tile(const TwoPassDesc& D, const Passes&
   __syncthreads();
   int span = L;
   for (int j = 0, seg = 0; j < P.m; ++j) {
-#if LNT_COL_GROUP_SYNC
-    // each column's passes touch only that column: its own threads' barrier,
-    // the block's before the tile leaves shared memory
-    pass_r_grouped<0, MR>(P.radix[j], sm, ld, T, L, span, D.itw2 + seg);
-    if (j + 1 < P.m) group_sync(T);
-    else __syncthreads();
-#else
     pass_r<0, MR>(P.radix[j], sm, ld, T, L, span, D.itw2 + seg);
     __syncthreads();
-#endif
     seg += span;
     span /= P.radix[j];
   }
@@ -396,14 +397,8 @@ __device__ __forceinline__ void inverse_tile(const TwoPassDesc& D, const Passes&
   int span = 1;
   for (int j = P.m - 1; j >= 0; --j) {
     span *= P.radix[j];
-#if LNT_COL_GROUP_SYNC
-    pass_r_grouped<1, MR>(P.radix[j], sm, ld, T, L, span, D.iitw2 + pass_table_offset(P, L, j));
-    if (j > 0) group_sync(T);
-    else __syncthreads();  // the carry step reads every column of a row
-#else
     pass_r<1, MR>(P.radix[j], sm, ld, T, L, span, D.iitw2 + pass_table_offset(P, L, j));
     __syncthreads();
-#endif
   }
   for (int r = threadIdx.x; r < L; r += blockDim.x) {
     const size_t run = (size_t)t0 * L + r;
@@ -423,7 +418,7 @@ __device__ __forceinline__ void inverse_tile(const TwoPassDesc& D, const Passes&
 }
 
 template <int T, int TH, int MR>
-__global__ void __launch_bounds__(TH, TH == col_threads<T>() ? col_min_blocks<T, MR>() : 1) col_forward_r16(
+__global__ void __launch_bounds__(TH, col_min_blocks<TH, MR>()) col_forward_r16(
     const TwoPassDesc* __restrict__ Ds, Passes P, int apply_carries) {
   extern __shared__ __align__(16) uint64_t sm[];
   const TwoPassDesc& D = Ds[blockIdx.y];
@@ -436,7 +431,7 @@ __global__ void __launch_bounds__(TH, TH == col_threads<T>() ? col_min_blocks<T,
 }
 
 template <int T, int TH, int MR>
-__global__ void __launch_bounds__(TH, TH == col_threads<T>() ? col_min_blocks<T, MR>() : 1) col_inverse_r16(
+__global__ void __launch_bounds__(TH, col_min_blocks<TH, MR>()) col_inverse_r16(
     const TwoPassDesc* __restrict__ Ds, Passes P, int unsigned_mode) {
   extern __shared__ __align__(16) uint64_t sm[];
   const TwoPassDesc& D = Ds[blockIdx.y];
@@ -507,7 +502,7 @@ __device__ __forceinline__ void wait_flag(const uint32_t* flag, uint32_t want, u
 }
 
 template <int T, int TH, int MR>
-__global__ void __launch_bounds__(TH, TH == col_threads<T>() ? col_min_blocks<T, MR>() : 1) col_fused_r16(
+__global__ void __launch_bounds__(TH, col_min_blocks<TH, MR>()) col_fused_r16(
     const TwoPassDesc* __restrict__ Ds, Passes P) {
   extern __shared__ __align__(16) uint64_t sm[];
   __shared__ uint32_t s_ticket, s_epoch;
@@ -583,11 +578,16 @@ cudaError_t ensure_smem(K* kernel, size_t smem) {
   return e;
 }
 
-int row_rows_per_cta(int L, int n2) {
+// Rows per row-kernel CTA: up to 4096 words of rows (the CTA's 256 threads
+// then have two tasks each per pass), fewer while the launch would have fewer
+// CTAs than the GPU has SMs (one test: latency) or than four per SM (a batch
+// of `count` tests: throughput).
+int row_rows_per_cta(int L, int n2, uint32_t count) {
   int rows = 4096 / L;
   if (rows < 1) rows = 1;
   const int sms = (int)device_sms();
-  while (rows > 1 && n2 / rows < sms) rows /= 2;
+  const long want = count > 1 ? 4L * sms : sms;
+  while (rows > 1 && (long)(n2 / rows) * (long)count < want) rows /= 2;
   return rows;
 }
 
@@ -625,7 +625,7 @@ inline int radix_log2(const TwoPassDesc& d) { return d.radix == 16 ? 4 : 3; }
 
 template <int TH, int MR>
 cudaError_t row_square_t(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count, cudaStream_t s) {
-  const int L = (int)d.n1, rows = row_rows_per_cta(L, (int)d.n2);
+  const int L = (int)d.n1, rows = row_rows_per_cta(L, (int)d.n2, count);
   const size_t smem = (size_t)rows * padded(L) * 8;
   cudaError_t e = ensure_smem(row_square_r16<TH, MR>, smem);
   if (e != cudaSuccess) return e;
@@ -636,7 +636,7 @@ cudaError_t row_square_t(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t c
 
 template <int TH, int MR>
 cudaError_t row_forward_t(const TwoPassDesc& d, const TwoPassDesc* dd, cudaStream_t s) {
-  const int L = (int)d.n1, rows = row_rows_per_cta(L, (int)d.n2);
+  const int L = (int)d.n1, rows = row_rows_per_cta(L, (int)d.n2, 1);
   const size_t smem = (size_t)rows * padded(L) * 8;
   cudaError_t e = ensure_smem(row_forward_r16<TH, MR>, smem);
   if (e != cudaSuccess) return e;
@@ -647,7 +647,7 @@ cudaError_t row_forward_t(const TwoPassDesc& d, const TwoPassDesc* dd, cudaStrea
 
 template <int TH, int MR>
 cudaError_t row_mul_t(const TwoPassDesc& d, const TwoPassDesc* dd, const uint64_t* F, cudaStream_t s) {
-  const int L = (int)d.n1, rows = row_rows_per_cta(L, (int)d.n2);
+  const int L = (int)d.n1, rows = row_rows_per_cta(L, (int)d.n2, 1);
   const size_t smem = (size_t)rows * padded(L) * 8;
   cudaError_t e = ensure_smem(row_mul_r16<TH, MR>, smem);
   if (e != cudaSuccess) return e;
@@ -676,7 +676,11 @@ cudaError_t row_mul_m(const TwoPassDesc& d, const TwoPassDesc* dd, const uint64_
 
 template <int MR>
 cudaError_t row_square_m(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count, cudaStream_t s) {
-  switch (row_threads_for((int)d.n1)) {
+  const int rows = row_rows_per_cta((int)d.n1, (int)d.n2, count);
+  switch (row_square_threads((int)d.n1, rows)) {
+    case 32: return row_square_t<32, MR>(d, dd, count, s);
+    case 64: return row_square_t<64, MR>(d, dd, count, s);
+    case 128: return row_square_t<128, MR>(d, dd, count, s);
     case 256: return row_square_t<256, MR>(d, dd, count, s);
     case 512: return row_square_t<512, MR>(d, dd, count, s);
     default: return row_square_t<1024, MR>(d, dd, count, s);
@@ -697,10 +701,20 @@ cudaError_t launch_row_square_r16(const TwoPassDesc& d, const TwoPassDesc* dd, u
   return d.radix == 16 ? row_square_m<16>(d, dd, count, s) : row_square_m<8>(d, dd, count, s);
 }
 
-// Columns of 4096 words hold one CTA per SM: 1024 threads instead of 128 per column.
-template <int T>
-constexpr int col_wide_threads() { return 1024; }
-
+// The column kernels' thread count for a tile of T columns of n2 words.
+template <int T, class F>
+cudaError_t col_dispatch(uint32_t n2, F&& f) {
+  switch (T * col_tpc(n2)) {
+    case 128:
+      if constexpr (T == 4) return f(std::integral_constant<int, 128>{});
+      break;
+    case 256: return f(std::integral_constant<int, 256>{});
+    case 512: return f(std::integral_constant<int, 512>{});
+    case 1024: return f(std::integral_constant<int, 1024>{});
+    default: break;
+  }
+  return cudaErrorInvalidConfiguration;
+}
 template <int T, int TH, int MR>
 cudaError_t col_forward_t(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count, bool apply,
                           cudaStream_t s) {
@@ -738,17 +752,17 @@ cudaError_t col_fused_t(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t co
 // CTAs the GPU holds at once.
 constexpr uint32_t kFusedTestsPerLaunch = 1024;
 
+template <int T, int MR>
+cudaError_t col_fused_tm(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count, cudaStream_t s) {
+  return col_dispatch<T>(d.n2, [&](auto th) { return col_fused_t<T, decltype(th)::value, MR>(d, dd, count, s); });
+}
+
 template <int MR>
 cudaError_t col_fused_m(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count, cudaStream_t s) {
   for (uint32_t first = 0; first < count; first += kFusedTestsPerLaunch) {
     const uint32_t c = count - first < kFusedTestsPerLaunch ? count - first : kFusedTestsPerLaunch;
-    cudaError_t e;
-    if (d.tile == 8)
-      e = col_fused_t<8, col_threads<8>(), MR>(d, dd + first, c, s);
-    else if (d.n2 >= 4096)
-      e = col_fused_t<4, col_wide_threads<4>(), MR>(d, dd + first, c, s);
-    else
-      e = col_fused_t<4, col_threads<4>(), MR>(d, dd + first, c, s);
+    const cudaError_t e = d.tile == 8 ? col_fused_tm<8, MR>(d, dd + first, c, s)
+                                      : col_fused_tm<4, MR>(d, dd + first, c, s);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -757,17 +771,21 @@ cudaError_t col_fused_m(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t co
 template <int MR>
 cudaError_t col_forward_m(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count, bool apply,
                           cudaStream_t s) {
-  if (d.tile == 8) return col_forward_t<8, col_threads<8>(), MR>(d, dd, count, apply, s);
-  if (d.n2 >= 4096) return col_forward_t<4, col_wide_threads<4>(), MR>(d, dd, count, apply, s);
-  return col_forward_t<4, col_threads<4>(), MR>(d, dd, count, apply, s);
+  if (d.tile == 8)
+    return col_dispatch<8>(d.n2, [&](auto th) { return col_forward_t<8, decltype(th)::value, MR>(d, dd, count, apply, s); });
+  return col_dispatch<4>(d.n2, [&](auto th) { return col_forward_t<4, decltype(th)::value, MR>(d, dd, count, apply, s); });
 }
 
 template <int MR>
 cudaError_t col_inverse_m(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
                           bool unsigned_mode, cudaStream_t s) {
-  if (d.tile == 8) return col_inverse_t<8, col_threads<8>(), MR>(d, dd, count, unsigned_mode, s);
-  if (d.n2 >= 4096) return col_inverse_t<4, col_wide_threads<4>(), MR>(d, dd, count, unsigned_mode, s);
-  return col_inverse_t<4, col_threads<4>(), MR>(d, dd, count, unsigned_mode, s);
+  if (d.tile == 8)
+    return col_dispatch<8>(d.n2, [&](auto th) {
+      return col_inverse_t<8, decltype(th)::value, MR>(d, dd, count, unsigned_mode, s);
+    });
+  return col_dispatch<4>(d.n2, [&](auto th) {
+    return col_inverse_t<4, decltype(th)::value, MR>(d, dd, count, unsigned_mode, s);
+  });
 }
 
 cudaError_t launch_col_fused_r16(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,

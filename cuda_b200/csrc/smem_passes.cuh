@@ -180,59 +180,6 @@ __device__ __forceinline__ void pass_tasks(uint64_t* sm, int ld, int ntrans, int
   }
 }
 
-// Column-affine variant for column tiles: the block's threads split into
-// `ntrans` equal groups, group g works on transform g only, so a pass needs a
-// barrier among its group's warps (named barrier 1 + g) instead of the whole
-// block's.
-template <int R, int Mode, bool Big>
-__device__ __forceinline__ void pass_tasks_grouped(uint64_t* sm, int ld, int ntrans, int L, int span,
-                                                   const uint64_t* tw) {
-  const int q = span / R, per = L / R, qs = q + (q >> 4);
-  const int lq = __ffs(q) - 1;
-  const int tpg = blockDim.x / ntrans, g = threadIdx.x / tpg;
-  uint64_t* base = sm + g * ld;
-  for (int k = threadIdx.x - g * tpg; k < per; k += tpg) {
-    const int b = k >> lq, t = k & (q - 1);
-    if constexpr (Mode == 0)
-      task_dif<R, Big>(base, sw(b * span + t), q, qs, tw + t * R);
-    else
-      task_dit<R, Big>(base, sw(b * span + t), q, qs, tw + t * R);
-  }
-}
-
-// Barrier among the threads of group g of `ntrans` equal groups (bar.sync with
-// id 1 + g; id 0 is __syncthreads').  Every thread of the group's warps arrives.
-__device__ __forceinline__ void group_sync(int ntrans) {
-  const int tpg = blockDim.x / ntrans, g = threadIdx.x / tpg;
-  asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(tpg) : "memory");
-}
-
-template <int Mode, int MR = kMaxRadix>
-__device__ __forceinline__ void pass_r_grouped(int R, uint64_t* sm, int ld, int ntrans, int L, int span,
-                                               const uint64_t* tw) {
-  const bool big = span / R >= 16;
-  switch (R) {
-    case 2:
-      big ? pass_tasks_grouped<2, Mode, true>(sm, ld, ntrans, L, span, tw)
-          : pass_tasks_grouped<2, Mode, false>(sm, ld, ntrans, L, span, tw);
-      break;
-    case 4:
-      big ? pass_tasks_grouped<4, Mode, true>(sm, ld, ntrans, L, span, tw)
-          : pass_tasks_grouped<4, Mode, false>(sm, ld, ntrans, L, span, tw);
-      break;
-    case 8:
-      big ? pass_tasks_grouped<8, Mode, true>(sm, ld, ntrans, L, span, tw)
-          : pass_tasks_grouped<8, Mode, false>(sm, ld, ntrans, L, span, tw);
-      break;
-    default:
-      if constexpr (MR >= 16) {
-        big ? pass_tasks_grouped<16, Mode, true>(sm, ld, ntrans, L, span, tw)
-            : pass_tasks_grouped<16, Mode, false>(sm, ld, ntrans, L, span, tw);
-      }
-      break;
-  }
-}
-
 // A pass over `ntrans` transforms of length L; transform g lives at sm + g * ld.
 // tw: this pass's part of the pass table.
 // Mode 0: DIF, 1: DIT, 2: square, 3: product with the transformed rows at tw

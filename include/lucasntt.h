@@ -321,6 +321,11 @@ int lnt_batch_pending(lnt_batch* b, uint32_t* pending);
  * carry-run class) for the batch's lifetime; 0 (default): policy plans. */
 int lnt_batch_autotune(lnt_batch* b, uint32_t loops);
 
+/* tests > 1: the autotuner times each candidate plan on `tests` copies of the
+ * test advancing together in a scratch batch (the batched launches the real
+ * groups run) instead of one test alone; 1 (default): alone. */
+int lnt_batch_autotune_group(lnt_batch* b, uint32_t tests);
+
 /* enable != 0 (default): grouped squarings replay a captured CUDA graph of
  * 8 squarings of every group; 0: plain stream launches. */
 int lnt_batch_use_graphs(lnt_batch* b, int enable);
