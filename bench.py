@@ -65,6 +65,8 @@ def parse_args():
                     help="c3/c4: plain path run test by test, or summed from per-length times")
     ap.add_argument("--rates", default="0.25,1", help="c5: arrival rates, requests per second")
     ap.add_argument("--drain", type=float, default=60.0, help="c5: seconds the engine runs on after the window")
+    ap.add_argument("--step-seconds", type=float, default=0.25,
+                    help="c5: time budget of one engine call (iteration-level scheduling; 0: lockstep)")
     ap.add_argument("--c5-range", default="10000,30000000", help="c5: exponent range")
     return ap.parse_args()
 
@@ -581,7 +583,11 @@ def run_serving(args, rank=0, world=1, local_rank=0):
     percentiles, which the line says.  The plain path is the same arrivals
     served one at a time in arrival order (FIFO) with service times = squarings
     x this repository's single-test µs per squaring at the request's length
-    (measured once per length): a simulation, labelled as one.  Every finished
+    (measured once per length): a simulation, labelled as one.  Each engine
+    call has a time budget (--step-seconds, lnt_batch_step_seconds): every
+    launch group and resident test runs as many squarings as fit in it at its
+    own pace, so new requests are admitted and finished ones retired about that
+    often, and small tests are not held to the pace of large ones.  Every finished
     request whose full-test Res64 the reference build has is compared with it.
     With N ranks the stream's rate is N times higher and request i goes to rank
     i mod N (round-robin dispatch to one engine per GPU)."""
@@ -620,7 +626,7 @@ def run_serving(args, rank=0, world=1, local_rank=0):
         work_done = 0.0
         if dist is not None:
             dist.barrier()
-        with cuda_b200.Batch(device=local_rank, hbm_budget_bytes=budget) as b:
+        with cuda_b200.Batch(device=local_rank, hbm_budget_bytes=budget, step_seconds=args.step_seconds) as b:
             t0 = time.perf_counter()
             k, info = 0, {}
             stop = args.seconds + args.drain
@@ -635,7 +641,7 @@ def run_serving(args, rank=0, world=1, local_rank=0):
                 if not info:  # nothing in flight: wait for the next arrival
                     time.sleep(max(0.0, min(mine[k][0] - now, 0.05)))
                     continue
-                b.run(args.batch_step)
+                b.run(args.batch_step if args.step_seconds <= 0 else 1 << 40)
                 now = time.perf_counter() - t0
                 for r in b.poll():
                     ta, q, prp = info.pop(r["id"])
@@ -690,6 +696,7 @@ def run_serving(args, rank=0, world=1, local_rank=0):
                 "config": {"exponents": f"seeded pool of 64: q log-uniform in [{lo}, {hi}], LL/PRP by a "
                                         "fair coin (random.Random(2))", "window_s": args.seconds,
                            "drain_s": args.drain, "hbm_budget_gb": 150, "arrival": "Poisson",
+                           "engine_call_budget_s": args.step_seconds,
                            "dispatch": "round-robin over ranks" if world > 1 else "one engine"}}
         print(json.dumps(line), flush=True)
         if bad:

@@ -122,6 +122,7 @@ def lib() -> ctypes.CDLL:
         "lnt_batch_use_graphs": ([vp, i32], i32),
         "lnt_batch_checkpoint_every": ([vp, u64], i32),
         "lnt_batch_autotune_group": ([vp, u32], i32),
+        "lnt_batch_step_seconds": ([vp, ctypes.c_double], i32),
         "lnt_batch_poll_checkpoints": ([vp, ctypes.POINTER(BatchCheckpoint), i32, ctypes.POINTER(i32)], i32),
         "lnt_batch_plan_cache": ([vp, cp], i32),
         "lnt_arith_selftest": ([i32, ctypes.POINTER(u64), ctypes.POINTER(u64)], i32),
@@ -327,7 +328,7 @@ class Batch:
 
     def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, autotune_loops: int = 0,
                  graphs: bool = True, checkpoint_every: int = 0, plan_cache: str | None = None,
-                 autotune_group: int = 1):
+                 autotune_group: int = 1, step_seconds: float = 0.0):
         h = ctypes.c_void_p()
         _check(lib().lnt_batch_create(device, int(hbm_budget_bytes), ctypes.byref(h)), "lnt_batch_create")
         self._h = h
@@ -339,6 +340,8 @@ class Batch:
             _check(lib().lnt_batch_autotune_group(self._h, int(autotune_group)), "lnt_batch_autotune_group")
         if checkpoint_every:
             _check(lib().lnt_batch_checkpoint_every(self._h, int(checkpoint_every)), "lnt_batch_checkpoint_every")
+        if step_seconds:
+            _check(lib().lnt_batch_step_seconds(self._h, float(step_seconds)), "lnt_batch_step_seconds")
         if not graphs:
             _check(lib().lnt_batch_use_graphs(self._h, 0), "lnt_batch_use_graphs")
 

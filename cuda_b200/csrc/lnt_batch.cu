@@ -82,6 +82,9 @@ struct Group {
   size_t cap = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t join = nullptr;  // recorded on `stream` after the group's launches
+  cudaEvent_t t0 = nullptr, t1 = nullptr;  // around the group's squarings of a call
+  cudaGraphExec_t graph = nullptr;  // kGraphChunk squarings, captured on `stream`
+  uint64_t k = 0;                   // squarings of the current call
 };
 
 int berr(int status, const std::string& msg) {
@@ -109,9 +112,14 @@ struct lnt_batch {
   std::vector<cudaStream_t> spare_streams;
   cudaStream_t rstream = nullptr;    // the resident launch, beside the groups
   cudaEvent_t fork = nullptr;        // recorded on `stream` before the group launches
-  // graph of kGraphChunk squarings of every group, valid until membership changes
-  cudaGraphExec_t graph = nullptr;
+  cudaEvent_t r0 = nullptr, r1 = nullptr;  // around the resident launch
   bool use_graphs = true;
+  // per-call time budget (lnt_batch_step_seconds; 0: every group advances in lockstep) and the
+  // measured seconds per squaring per test of each group geometry, and per word-squaring of
+  // the resident launch, that it is split by
+  double step_seconds = 0;
+  std::map<GroupKey, double> group_rate;
+  double resident_rate = 0;
   // autotuned plans: (n, shortest valid run) -> plan; loops = 0: policy plans
   uint32_t tune_loops = 0;
   uint32_t tune_group = 1;  // tests timed together per candidate plan (1: one test alone)
@@ -155,68 +163,93 @@ cudaStream_t take_stream(lnt_batch* b) {
   return s;
 }
 
-void drop_graph(lnt_batch* b) {
-  if (b->graph) cudaGraphExecDestroy(b->graph);
-  b->graph = nullptr;
+void drop_graphs(lnt_batch* b) {
+  for (auto& kv : b->groups) {
+    if (kv.second.graph) cudaGraphExecDestroy(kv.second.graph);
+    kv.second.graph = nullptr;
+  }
 }
 
-// One chunk of squarings of every group, forked from b->stream onto the group
-// streams and joined back (the body of the captured graph).
-int launch_groups(lnt_batch* b, uint64_t k) {
+// k squarings of one group on its stream.
+int group_launches(Group& g, uint64_t k) {
+  const uint32_t cnt = (uint32_t)g.members.size();
+  if (!g.fused) {
+    for (uint64_t it = 0; it < k; ++it) {
+      BCUDA(lnt::launch_col_forward_r16(g.geometry, g.d_descs, cnt, true, g.stream), "col_forward");
+      BCUDA(lnt::launch_row_square_r16(g.geometry, g.d_descs, cnt, g.stream), "row_square");
+      BCUDA(lnt::launch_col_inverse_r16(g.geometry, g.d_descs, cnt, false, g.stream), "col_inverse");
+    }
+  } else if (k > 0) {
+    // col_forward, row, (fused col_inverse + col_forward, row) x (k - 1), col_inverse
+    BCUDA(lnt::launch_col_forward_r16(g.geometry, g.d_descs, cnt, true, g.stream), "col_forward");
+    BCUDA(lnt::launch_row_square_r16(g.geometry, g.d_descs, cnt, g.stream), "row_square");
+    for (uint64_t it = 1; it < k; ++it) {
+      BCUDA(lnt::launch_col_fused_r16(g.geometry, g.d_descs, cnt, g.stream), "col_fused");
+      BCUDA(lnt::launch_row_square_r16(g.geometry, g.d_descs, cnt, g.stream), "row_square");
+    }
+    BCUDA(lnt::launch_col_inverse_r16(g.geometry, g.d_descs, cnt, false, g.stream), "col_inverse");
+  }
+  return LNT_OK;
+}
+
+// The group's kGraphChunk squarings captured once per membership and replayed.
+int build_group_graph(Group& g) {
+  BCUDA(cudaStreamBeginCapture(g.stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+  const int st = group_launches(g, kGraphChunk);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(g.stream, &graph);
+  if (st != LNT_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return st;
+  }
+  if (e != cudaSuccess) return berr(LNT_ERR_CUDA, std::string("end capture: ") + cudaGetErrorString(e));
+  const cudaError_t ie = cudaGraphInstantiate(&g.graph, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ie != cudaSuccess) {
+    g.graph = nullptr;
+    return berr(LNT_ERR_CUDA, std::string("instantiate graph: ") + cudaGetErrorString(ie));
+  }
+  return LNT_OK;
+}
+
+// Every group's g.k squarings, forked from b->stream onto the group streams
+// (graph replays of kGraphChunk squarings, the remainder as plain launches)
+// and joined back; events around each group's work time it.
+int launch_groups(lnt_batch* b) {
   BCUDA(cudaEventRecord(b->fork, b->stream), "fork");
   for (auto& kv : b->groups) {
     Group& g = kv.second;
-    const uint32_t cnt = (uint32_t)g.members.size();
     BCUDA(cudaStreamWaitEvent(g.stream, b->fork, 0), "fork wait");
-    if (!g.fused) {
-      for (uint64_t it = 0; it < k; ++it) {
-        BCUDA(lnt::launch_col_forward_r16(g.geometry, g.d_descs, cnt, true, g.stream), "col_forward");
-        BCUDA(lnt::launch_row_square_r16(g.geometry, g.d_descs, cnt, g.stream), "row_square");
-        BCUDA(lnt::launch_col_inverse_r16(g.geometry, g.d_descs, cnt, false, g.stream), "col_inverse");
+    BCUDA(cudaEventRecord(g.t0, g.stream), "group timer");
+    uint64_t left = g.k;
+    if (b->use_graphs && left >= kGraphChunk) {
+      if (!g.graph) {
+        const int st = build_group_graph(g);
+        if (st != LNT_OK) return st;
       }
-    } else if (k > 0) {
-      // col_forward, row, (fused col_inverse + col_forward, row) x (k - 1), col_inverse
-      BCUDA(lnt::launch_col_forward_r16(g.geometry, g.d_descs, cnt, true, g.stream), "col_forward");
-      BCUDA(lnt::launch_row_square_r16(g.geometry, g.d_descs, cnt, g.stream), "row_square");
-      for (uint64_t it = 1; it < k; ++it) {
-        BCUDA(lnt::launch_col_fused_r16(g.geometry, g.d_descs, cnt, g.stream), "col_fused");
-        BCUDA(lnt::launch_row_square_r16(g.geometry, g.d_descs, cnt, g.stream), "row_square");
-      }
-      BCUDA(lnt::launch_col_inverse_r16(g.geometry, g.d_descs, cnt, false, g.stream), "col_inverse");
+      for (; left >= kGraphChunk; left -= kGraphChunk) BCUDA(cudaGraphLaunch(g.graph, g.stream), "graph launch");
     }
+    const int st = group_launches(g, left);
+    if (st != LNT_OK) return st;
+    BCUDA(cudaEventRecord(g.t1, g.stream), "group timer");
     BCUDA(cudaEventRecord(g.join, g.stream), "join");
     BCUDA(cudaStreamWaitEvent(b->stream, g.join, 0), "join wait");
   }
   return LNT_OK;
 }
 
-int build_graph(lnt_batch* b) {
-  drop_graph(b);
-  BCUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-  const int st = launch_groups(b, kGraphChunk);
-  cudaGraph_t g = nullptr;
-  const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
-  if (st != LNT_OK) {
-    if (g) cudaGraphDestroy(g);
-    return st;
-  }
-  if (e != cudaSuccess) return berr(LNT_ERR_CUDA, std::string("end capture: ") + cudaGetErrorString(e));
-  const cudaError_t ie = cudaGraphInstantiate(&b->graph, g, 0);
-  cudaGraphDestroy(g);
-  if (ie != cudaSuccess) {
-    b->graph = nullptr;
-    return berr(LNT_ERR_CUDA, std::string("instantiate graph: ") + cudaGetErrorString(ie));
-  }
-  return LNT_OK;
+void free_group(lnt_batch* b, Group& g, bool keep_stream) {
+  if (g.graph) cudaGraphExecDestroy(g.graph);
+  if (g.d_descs) cudaFree(g.d_descs);
+  for (cudaEvent_t e : {g.join, g.t0, g.t1})
+    if (e) cudaEventDestroy(e);
+  if (keep_stream) b->spare_streams.push_back(g.stream);
+  else if (g.stream) cudaStreamDestroy(g.stream);
+  g = Group();
 }
 
 int rebuild(lnt_batch* b) {
-  drop_graph(b);
-  for (auto& kv : b->groups) {
-    if (kv.second.d_descs) cudaFree(kv.second.d_descs);
-    if (kv.second.join) cudaEventDestroy(kv.second.join);
-    b->spare_streams.push_back(kv.second.stream);
-  }
+  for (auto& kv : b->groups) free_group(b, kv.second, true);
   b->groups.clear();
   b->resident.clear();
   b->singles.clear();
@@ -248,6 +281,8 @@ int rebuild(lnt_batch* b) {
     BCUDA(cudaDeviceSynchronize(), "synchronize");
     g.stream = take_stream(b);
     BCUDA(cudaEventCreateWithFlags(&g.join, cudaEventDisableTiming), "group event");
+    BCUDA(cudaEventCreate(&g.t0), "group event");
+    BCUDA(cudaEventCreate(&g.t1), "group event");
   }
   if (b->resident.size() > b->rcap) {
     if (b->d_rdescs) cudaFree(b->d_rdescs);
@@ -308,9 +343,12 @@ int lnt_batch_create(int device, uint64_t hbm_budget_bytes, lnt_batch** out) {
   b->budget = hbm_budget_bytes;
   if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&b->rstream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess) {
+      cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreate(&b->r0) != cudaSuccess || cudaEventCreate(&b->r1) != cudaSuccess) {
     if (b->stream) cudaStreamDestroy(b->stream);
     if (b->rstream) cudaStreamDestroy(b->rstream);
+    for (cudaEvent_t e : {b->fork, b->r0, b->r1})
+      if (e) cudaEventDestroy(e);
     delete b;
     return berr(LNT_ERR_CUDA, "cudaStreamCreate");
   }
@@ -322,14 +360,10 @@ int lnt_batch_destroy(lnt_batch* b) {
   if (!b) return LNT_OK;
   DeviceGuard guard(b->device);
   cudaDeviceSynchronize();
-  drop_graph(b);
   for (auto& e : b->active) lnt_destroy(e.t);
-  for (auto& kv : b->groups) {
-    if (kv.second.d_descs) cudaFree(kv.second.d_descs);
-    if (kv.second.join) cudaEventDestroy(kv.second.join);
-    if (kv.second.stream) cudaStreamDestroy(kv.second.stream);
-  }
-  if (b->fork) cudaEventDestroy(b->fork);
+  for (auto& kv : b->groups) free_group(b, kv.second, false);
+  for (cudaEvent_t e : {b->fork, b->r0, b->r1})
+    if (e) cudaEventDestroy(e);
   for (cudaStream_t s : b->spare_streams)
     if (s) cudaStreamDestroy(s);
   if (b->d_rdescs) cudaFree(b->d_rdescs);
@@ -598,42 +632,74 @@ int lnt_batch_run(lnt_batch* b, uint64_t iterations) {
   record_checkpoints(b);  // tests admitted at a checkpoint (their first squaring runs at admission)
   if (b->active.empty() || iterations == 0) return LNT_OK;
   if (b->dirty && (st = rebuild(b)) != LNT_OK) return st;
+  const bool budget = b->step_seconds > 0;
   // squarings test i may run in this call: up to its target and its next checkpoint
   std::vector<uint64_t> step(b->active.size());
   for (size_t i = 0; i < b->active.size(); ++i) step[i] = std::min(iterations, steps_left(b, b->active[i]));
-  // grouped tests advance in lockstep: no test of a group may pass its target or checkpoint
-  uint64_t k = iterations;
+  // a group's tests advance together, none past its target or checkpoint.  Without a
+  // time budget every group runs the same count (lockstep); with one, each group runs
+  // as many squarings as fit in the budget at its measured (at first, modelled) pace
+  uint64_t lockstep = iterations;
   for (auto& kv : b->groups)
-    for (size_t i : kv.second.members) k = std::min(k, step[i]);
-  for (auto& kv : b->groups)
-    for (size_t i : kv.second.members) step[i] = k;
+    for (size_t i : kv.second.members) lockstep = std::min(lockstep, step[i]);
+  for (auto& kv : b->groups) {
+    Group& g = kv.second;
+    uint64_t k = iterations;
+    for (size_t i : g.members) k = std::min(k, step[i]);
+    if (!budget) {
+      k = lockstep;
+    } else {
+      auto r = b->group_rate.find(kv.first);
+      const double per_test = r != b->group_rate.end() ? r->second : 60e-12 * g.n + 2e-6;
+      const double sq = per_test * (double)g.members.size() + 10e-6;
+      k = std::min<uint64_t>(k, std::max<uint64_t>(1, (uint64_t)(b->step_seconds / sq)));
+    }
+    g.k = k;
+    for (size_t i : g.members) step[i] = k;
+  }
   // SMEM-resident tests: one launch, per-test counts, beside the groups
+  uint64_t resident_work = 0;  // word-squarings of the slowest CTA
   if (!b->resident.empty()) {
     std::vector<lnt::ResidentDesc> h;
     uint32_t max_n = 0;
+    const double rate = b->resident_rate > 0 ? b->resident_rate : 5e-9;
     for (size_t i : b->resident) {
       Entry& e = b->active[i];
+      if (budget)
+        step[i] = std::min<uint64_t>(step[i], std::max<uint64_t>(1, (uint64_t)(b->step_seconds / (rate * e.n))));
       h.push_back(lnt::test_resident_desc(e.t, step[i]));
       max_n = std::max(max_n, e.n);
+      resident_work = std::max<uint64_t>(resident_work, step[i] * e.n);
     }
     BCUDA(cudaMemcpyAsync(b->d_rdescs, h.data(), h.size() * sizeof(lnt::ResidentDesc),
                           cudaMemcpyHostToDevice, b->rstream),
           "upload resident descriptors");
+    BCUDA(cudaEventRecord(b->r0, b->rstream), "resident timer");
     BCUDA(lnt::launch_resident(b->d_rdescs, (uint32_t)h.size(), max_n, b->rstream), "resident kernel");
+    BCUDA(cudaEventRecord(b->r1, b->rstream), "resident timer");
   }
-  if (!b->groups.empty() && k > 0) {
-    uint64_t left = k;
-    if (b->use_graphs && k >= kGraphChunk) {
-      if (!b->graph && (st = build_graph(b)) != LNT_OK) return st;
-      for (; left >= kGraphChunk; left -= kGraphChunk)
-        BCUDA(cudaGraphLaunch(b->graph, b->stream), "graph launch");
-    }
-    if (left && (st = launch_groups(b, left)) != LNT_OK) return st;
-  }
+  if (!b->groups.empty() && (st = launch_groups(b)) != LNT_OK) return st;
   for (size_t i : b->singles) {
     if ((st = lnt_iterate(b->active[i].t, step[i])) != LNT_OK) return st;
   }
   BCUDA(cudaDeviceSynchronize(), "synchronize");
+  // paces for the next budgeted call (smoothed)
+  for (auto& kv : b->groups) {
+    Group& g = kv.second;
+    float ms = 0;
+    if (g.k >= kGraphChunk && cudaEventElapsedTime(&ms, g.t0, g.t1) == cudaSuccess && ms > 0) {
+      const double per_test = ms * 1e-3 / ((double)g.k * (double)g.members.size());
+      auto r = b->group_rate.find(kv.first);
+      b->group_rate[kv.first] = r == b->group_rate.end() ? per_test : 0.5 * (r->second + per_test);
+    }
+  }
+  if (!b->resident.empty() && resident_work >= 8 * 512) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, b->r0, b->r1) == cudaSuccess && ms > 0) {
+      const double rate = ms * 1e-3 / (double)resident_work;
+      b->resident_rate = b->resident_rate > 0 ? 0.5 * (b->resident_rate + rate) : rate;
+    }
+  }
   for (size_t i : b->resident) {
     b->active[i].done += step[i];
     lnt::test_mark_iterated(b->active[i].t);
@@ -647,6 +713,13 @@ int lnt_batch_run(lnt_batch* b, uint64_t iterations) {
   record_checkpoints(b);
   if ((st = retire_finished(b)) != LNT_OK) return st;
   return admit_pending(b);
+}
+
+int lnt_batch_step_seconds(lnt_batch* b, double seconds) {
+  if (!b) return berr(LNT_ERR_INVALID_ARGUMENT, "null batch");
+  if (!(seconds >= 0)) return berr(LNT_ERR_INVALID_ARGUMENT, "seconds must be >= 0");
+  b->step_seconds = seconds;
+  return LNT_OK;
 }
 
 int lnt_batch_autotune(lnt_batch* b, uint32_t loops) {
@@ -690,7 +763,7 @@ int lnt_batch_use_graphs(lnt_batch* b, int enable) {
   if (!b) return berr(LNT_ERR_INVALID_ARGUMENT, "null batch");
   DeviceGuard guard(b->device);
   b->use_graphs = enable != 0;
-  if (!b->use_graphs) drop_graph(b);
+  if (!b->use_graphs) drop_graphs(b);
   return LNT_OK;
 }
 

@@ -30,12 +30,14 @@ using namespace smem;
 // 256 threads per row of up to 4096 words (four CTAs per SM); longer rows hold
 // one or two CTAs per SM, so their CTAs are wider to keep 32 warps per SM.
 constexpr int row_threads_for(int L) { return L <= 4096 ? 256 : (L == 8192 ? 512 : 1024); }
-// The squaring kernel's CTA for `rows` rows of L words: up to 4096 words take
-// two radix-8 tasks per thread per pass (256 threads for 4096 words, down to
-// one warp), longer rows as row_threads_for.
-constexpr int row_square_threads(int L, int rows) {
+// The squaring kernel's CTA for `rows` rows of L words: in a launch that fills
+// the GPU, up to 4096 words take two radix-8 tasks per thread per pass (256
+// threads for 4096 words, down to one warp); a launch of fewer CTAs than twice
+// the SMs (latency) keeps 256; longer rows as row_threads_for.
+constexpr int row_square_threads(int L, int rows, bool latency) {
   return L > 4096 ? row_threads_for(L)
-                  : (L * rows >= 4096 ? 256 : (L * rows >= 2048 ? 128 : (L * rows >= 1024 ? 64 : 32)));
+                  : (L * rows >= 4096 || latency ? 256
+                                                 : (L * rows >= 2048 ? 128 : (L * rows >= 1024 ? 64 : 32)));
 }
 #ifndef LNT_ROW_MIN_BLOCKS
 #define LNT_ROW_MIN_BLOCKS 4  // CTAs per SM the row kernel is compiled for (registers)
@@ -231,12 +233,18 @@ __global__ void __launch_bounds__(TH) row_mul_r16(const TwoPassDesc* __restrict_
 
 // --------------------------------------------------------------- columns ----
 
-// Threads per tile column: one per radix-8 task of a pass (n2 / 8), at least a
-// warp and at most 128, or 256 for columns of 4096 words (one 4-column CTA per
-// SM).  Short columns (small lengths) thus get small CTAs, many per SM, instead
-// of CTAs whose threads mostly idle.
-__host__ __device__ constexpr int col_tpc(uint32_t n2) {
-  return n2 >= 4096 ? 256 : (n2 >= 1024 ? 128 : (n2 == 512 ? 64 : 32));
+// Threads per tile column.  A launch with CTAs enough to fill the GPU
+// (throughput: a batch) gives each column one thread per radix-8 task of a pass
+// (n2 / 8), at least a warp and at most 128, or 256 for columns of 4096 words
+// (one 4-column CTA per SM): short columns then get small CTAs, many per SM,
+// instead of CTAs whose threads mostly idle.  A launch with fewer CTAs than
+// twice the SMs (one short test: latency) keeps 128 threads a column, whose
+// row-wise steps (carries, weights, staging) then run in parallel.
+__host__ __device__ constexpr int col_tpc(uint32_t n2, bool latency) {
+  return n2 >= 4096 ? 256 : (n2 >= 1024 || latency ? 128 : (n2 == 512 ? 64 : 32));
+}
+inline bool col_latency_mode(const TwoPassDesc& d, uint32_t count) {
+  return (uint64_t)d.ntiles * count < 2ull * device_sms();
 }
 // CTAs per SM the column kernels are compiled for: 64 registers a thread at
 // 1024 threads an SM (128 for radix-16 passes, which spill at 64)
@@ -677,7 +685,8 @@ cudaError_t row_mul_m(const TwoPassDesc& d, const TwoPassDesc* dd, const uint64_
 template <int MR>
 cudaError_t row_square_m(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count, cudaStream_t s) {
   const int rows = row_rows_per_cta((int)d.n1, (int)d.n2, count);
-  switch (row_square_threads((int)d.n1, rows)) {
+  const bool latency = (uint64_t)(d.n2 / rows) * count < 2ull * device_sms();
+  switch (row_square_threads((int)d.n1, rows, latency)) {
     case 32: return row_square_t<32, MR>(d, dd, count, s);
     case 64: return row_square_t<64, MR>(d, dd, count, s);
     case 128: return row_square_t<128, MR>(d, dd, count, s);
@@ -703,8 +712,8 @@ cudaError_t launch_row_square_r16(const TwoPassDesc& d, const TwoPassDesc* dd, u
 
 // The column kernels' thread count for a tile of T columns of n2 words.
 template <int T, class F>
-cudaError_t col_dispatch(uint32_t n2, F&& f) {
-  switch (T * col_tpc(n2)) {
+cudaError_t col_dispatch(uint32_t n2, bool latency, F&& f) {
+  switch (T * col_tpc(n2, latency)) {
     case 128:
       if constexpr (T == 4) return f(std::integral_constant<int, 128>{});
       break;
@@ -754,7 +763,8 @@ constexpr uint32_t kFusedTestsPerLaunch = 1024;
 
 template <int T, int MR>
 cudaError_t col_fused_tm(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count, cudaStream_t s) {
-  return col_dispatch<T>(d.n2, [&](auto th) { return col_fused_t<T, decltype(th)::value, MR>(d, dd, count, s); });
+  return col_dispatch<T>(d.n2, col_latency_mode(d, count),
+                         [&](auto th) { return col_fused_t<T, decltype(th)::value, MR>(d, dd, count, s); });
 }
 
 template <int MR>
@@ -771,19 +781,23 @@ cudaError_t col_fused_m(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t co
 template <int MR>
 cudaError_t col_forward_m(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count, bool apply,
                           cudaStream_t s) {
+  const bool latency = col_latency_mode(d, count);
   if (d.tile == 8)
-    return col_dispatch<8>(d.n2, [&](auto th) { return col_forward_t<8, decltype(th)::value, MR>(d, dd, count, apply, s); });
-  return col_dispatch<4>(d.n2, [&](auto th) { return col_forward_t<4, decltype(th)::value, MR>(d, dd, count, apply, s); });
+    return col_dispatch<8>(d.n2, latency,
+                           [&](auto th) { return col_forward_t<8, decltype(th)::value, MR>(d, dd, count, apply, s); });
+  return col_dispatch<4>(d.n2, latency,
+                         [&](auto th) { return col_forward_t<4, decltype(th)::value, MR>(d, dd, count, apply, s); });
 }
 
 template <int MR>
 cudaError_t col_inverse_m(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
                           bool unsigned_mode, cudaStream_t s) {
+  const bool latency = col_latency_mode(d, count);
   if (d.tile == 8)
-    return col_dispatch<8>(d.n2, [&](auto th) {
+    return col_dispatch<8>(d.n2, latency, [&](auto th) {
       return col_inverse_t<8, decltype(th)::value, MR>(d, dd, count, unsigned_mode, s);
     });
-  return col_dispatch<4>(d.n2, [&](auto th) {
+  return col_dispatch<4>(d.n2, latency, [&](auto th) {
     return col_inverse_t<4, decltype(th)::value, MR>(d, dd, count, unsigned_mode, s);
   });
 }

@@ -309,6 +309,14 @@ int lnt_batch_enqueue(lnt_batch* b, uint32_t exponent, uint32_t n, int prp, uint
  * tests admitted. */
 int lnt_batch_run(lnt_batch* b, uint64_t iterations);
 
+/* seconds > 0: each lnt_batch_run call gives every launch group (tests of one
+ * geometry) and every resident test as many squarings, up to `iterations`, as
+ * fit in about `seconds` at its measured pace, so a call takes about that long
+ * and small tests are not held to the pace of large ones (the serving loop's
+ * iteration-level scheduling); 0 (default): every test advances by the same
+ * count.  Results do not depend on it. */
+int lnt_batch_step_seconds(lnt_batch* b, double seconds);
+
 /* Move up to `cap` finished results to `out` (count in *count). */
 int lnt_batch_poll(lnt_batch* b, lnt_batch_result* out, int cap, int* count);
 

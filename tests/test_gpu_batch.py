@@ -231,3 +231,24 @@ def test_batch_keeps_plans_of_one_length_apart(lnt, tmp_path):
             got.update({r["id"]: r for r in b.poll()})
     for i, (q, prp) in ids.items():
         assert got[i]["status"] == 0 and got[i]["res64"] == alone(lnt, q, 0, prp, 30), (q, prp)
+
+
+def test_time_budgeted_calls_equal_alone(lnt):
+    """With a time budget per call (lnt_batch_step_seconds) each launch group and
+    each resident test runs its own number of squarings per call: a small test
+    is not held to the pace of a large one.  Residues equal the tests alone, and
+    the small resident test finishes in fewer calls than the 2^20-word test."""
+    tests = [(9941, 0, True, 2000), (160001, 0, False, 300), (12000017, 0, False, 400)]
+    calls = {}
+    with lnt.Batch(device=0, step_seconds=0.01) as b:
+        ids = {b.submit(q, n, prp, k): (q, n, prp, k) for q, n, prp, k in tests}
+        got, c = {}, 0
+        while len(got) < len(ids):
+            b.run(100000)
+            c += 1
+            for r in b.poll():
+                got[r["id"]] = r
+                calls[ids[r["id"]][0]] = c
+    for i, (q, n, prp, k) in ids.items():
+        assert got[i]["status"] == 0 and got[i]["res64"] == alone(lnt, q, n, prp, k), (q, prp)
+    assert calls[9941] < calls[12000017], calls
