@@ -95,8 +95,13 @@ def test_jacobi_check_ll(lnt):
     import ctypes
 
     L = lnt.lib()
+    L.lnt_jacobi_enable.argtypes = [ctypes.c_void_p, ctypes.c_uint64]
+    with lnt.LucasTest(9941, 0, False) as T:  # the SMEM-resident plan (no pending run carries)
+        assert T.plan.startswith("RESIDENT")
+        assert L.lnt_jacobi_enable(T._h, 1000) == 0, L.lnt_last_error()
+        T.iterate(9941 - 2)
+        assert T.is_prime()
     with lnt.LucasTest(132049, 0, False) as T:
-        L.lnt_jacobi_enable.argtypes = [ctypes.c_void_p, ctypes.c_uint64]
         assert L.lnt_jacobi_enable(T._h, 5000) == 0, L.lnt_last_error()
         T.iterate(132049 - 2)
         assert T.is_prime()
