@@ -393,6 +393,8 @@ def run_batch_workload(args, exps, prp, target_of, label, config, rank=0, world=
     # writes the plans to the cache, which the timed batch then loads
     tune_s = 0.0
     cache = args.plan_cache
+    if cache and world > 1:
+        cache = f"{cache}.rank{rank}"  # one file per process: the ranks tune and write concurrently
     if args.autotune_loops:
         import tempfile
 
