@@ -11,19 +11,24 @@
 // HBM budget and retired (Res64 and verdict recorded, memory released) as they
 // finish, so a caller can keep the engine full: continuous batching.
 //
-// The grouped launches of `kGraphChunk` squarings are captured once per group
-// membership into a CUDA graph (fork/join over the group streams) and replayed,
-// so a batch step costs one graph launch per chunk instead of 3 x groups x
-// chunk kernel launches.  Optionally (lnt_batch_autotune) each length's plan
-// (split, column tile) is picked by timing the candidates once per length,
-// the analogue of the reference's per-run autotune (process.cu:45-127).
+// Each group's launches of `kGraphChunk` squarings are captured once per group
+// membership into a CUDA graph on the group's stream and replayed, so a batch
+// step costs one graph launch per group and chunk instead of 3 x chunk kernel
+// launches.  Without a time budget every group advances by the same count per
+// call (lockstep); with one (lnt_batch_step_seconds) each group and resident
+// test runs as many squarings as fit in it at its measured pace.  Optionally
+// (lnt_batch_autotune) each length's plan (split, column tile, pass radix,
+// column fusion) is picked by timing the candidates once per length -- alone or
+// on a group of copies (lnt_batch_autotune_group) -- the analogue of the
+// reference's per-run autotune (process.cu:45-127), and kept in a JSON cache
+// (lnt_batch_plan_cache).  Res64 checkpoints every K squarings
+// (lnt_batch_checkpoint_every) record each test's intermediate residues.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
-#include <cstring>
 #include <deque>
 #include <fstream>
 #include <map>
