@@ -53,7 +53,7 @@ static void test_defaults() {
         o.env_filename == "LucasNTT_results.env");
   CHECK(o.dump_stats && !o.dump_residue && !o.dump_environment && !o.was_interrupted);
   CHECK(o.performance_loops == 500 && o.gpu == 0 && o.verbosity == Verbosity::Normal);
-  CHECK(o.gerbicz_block == 0);
+  CHECK(o.gerbicz_block == 0 && o.jacobi_interval == 0);
   CHECK(o.provided_length.empty() && o.preferred_pool.empty() && o.preferred_kernels == ";;");
 }
 
@@ -63,14 +63,14 @@ static void test_ini_and_argv() {
              "exponent = 44497\nPRP = 1\nIterations=1000\nperformanceloops = 77\n"
              "Verbosity = Silent\nGPU = 0\ndumpResidue = 1\ndumpStats = 0\ndumpEnvironment = 1\n"
              "Dump = r.dat\nStats = r.txt\nEnv = r.env\nfft = 4096\nPool = FFT_1SMEM\nKernels = a;b\n"
-             "GerbiczBlock = 64\n"
+             "GerbiczBlock = 64\nJacobiCheck = 250000\n"
              "[Section]\nExponent = 3\n");
   MainOptions o = resolve({});
   CHECK(o.exponent == 44497 && o.prp && o.iterations == 1000 && o.performance_loops == 77);
   CHECK(o.verbosity == Verbosity::Silent && o.dump_residue && !o.dump_stats && o.dump_environment);
   CHECK(o.dump_filename == "r.dat" && o.stat_filename == "r.txt" && o.env_filename == "r.env");
   CHECK(o.provided_length == "4096" && o.preferred_pool == "FFT_1SMEM" && o.preferred_kernels == ";a;b;");
-  CHECK(o.gerbicz_block == 64);
+  CHECK(o.gerbicz_block == 64 && o.jacobi_interval == 250000);
   // command line: exponent iterations prefix fft
   o = resolve({"9941", "50", "run1", "1024"});
   CHECK(o.exponent == 9941 && o.iterations == 50 && o.provided_length == "1024");

@@ -81,3 +81,18 @@ def test_register_ntt_host_build(tmp_path):
                     str(ROOT / "tests" / "native" / "ntt_selftest.cpp")], check=True)
     r = subprocess.run([str(exe)], capture_output=True, text=True)
     assert r.returncode == 0 and r.stdout.startswith("ok"), r.stdout
+
+
+def test_new_entry_points_reject_null_handles(lnt):
+    """The batch, plan-cache and Jacobi entry points return LNT_ERR_INVALID_ARGUMENT
+    (1) for a null handle instead of dereferencing it (no device needed)."""
+    L = lnt.lib()
+    assert L.lnt_batch_step_seconds(None, 0.25) == 1
+    assert L.lnt_batch_checkpoint_every(None, 100) == 1
+    assert L.lnt_batch_autotune_group(None, 8) == 1
+    assert L.lnt_batch_plan_cache(None, b"plans.json") == 1
+    assert L.lnt_batch_poll_checkpoints(None, None, 0, None) == 1
+    assert L.lnt_jacobi_enable(None, 1000) == 1
+    assert L.lnt_jacobi_check(None, None) == 1
+    assert L.lnt_jacobi_stats(None, None, None, None) == 1
+    assert L.lnt_jacobi_of_digits(None, None, 0, 0, None) == 1
