@@ -44,6 +44,7 @@ class BatchResult(ctypes.Structure):
 
 
 class BatchCheckpoint(ctypes.Structure):
+    """lnt_batch_checkpoint."""
     _fields_ = [("id", ctypes.c_uint64), ("iteration", ctypes.c_uint64), ("res64", ctypes.c_uint64),
                 ("status", ctypes.c_int)]
 
@@ -324,7 +325,14 @@ def test_device_bytes(exponent: int, n: int = 0) -> int:
 
 class Batch:
     """Many LL / PRP tests on one GPU, admitted under an HBM budget and retired
-    as they finish (lnt_batch_*)."""
+    as they finish (lnt_batch_*).
+
+    autotune_loops > 0 tunes each length's plan (lnt_batch_autotune), timing
+    each candidate on `autotune_group` tests together, and `plan_cache` keeps
+    the plans in a JSON file; checkpoint_every > 0 records Res64 checkpoints
+    (poll_checkpoints); step_seconds > 0 gives every run() call a time budget
+    split among the launch groups by their pace (lnt_batch_step_seconds);
+    graphs=False replaces the captured-graph replay by plain launches."""
 
     def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, autotune_loops: int = 0,
                  graphs: bool = True, checkpoint_every: int = 0, plan_cache: str | None = None,
