@@ -133,7 +133,8 @@ cudaError_t launch_col_forward(const TwoPassDesc& d, bool apply_carries, cudaStr
 cudaError_t launch_row_square(const TwoPassDesc& d, cudaStream_t s);
 cudaError_t launch_col_inverse(const TwoPassDesc& d, bool unsigned_mode, cudaStream_t s);
 
-// radix-16 pass variants (lnt_radix16.cu): n2 in [2^6, 2^12], n1 in [2^7, 2^12], n1 >= n2
+// register-pass kernels (lnt_radix16.cu, passes of radix up to 8 or 16): n2 in [2^6, 2^12],
+// n1 in [2^7, 2^14], n1 >= n2
 bool r16_supported(uint32_t log2n1, uint32_t log2n2);
 // radices of the passes of a length-2^log2L transform whose passes take at most
 // `radix` (8 or 16) points, first (largest span) first
