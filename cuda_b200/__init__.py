@@ -17,5 +17,6 @@ from .api import (  # noqa: F401
     plan_candidates,
     plan_describe,
     secured_log2_length,
+    shifted_words,
     test_device_bytes,
 )

@@ -85,6 +85,7 @@ def lib() -> ctypes.CDLL:
         "lnt_length_candidates": ([u32, cp, sz], i32),
         "lnt_parse_length": ([cp, ctypes.POINTER(u32)], i32),
         "lnt_check_provided_length": ([u32, cp, ctypes.POINTER(i32)], i32),
+        "lnt_shifted_words": ([u32, u32, ctypes.POINTER(u32), ctypes.POINTER(u32)], i32),
         "lnt_create": ([u32, u32, i32, i32, ctypes.POINTER(vp)], i32),
         "lnt_create_with_plan": ([u32, u32, i32, i32, ctypes.POINTER(PlanOptions), ctypes.POINTER(vp)], i32),
         "lnt_get_plan": ([vp, ctypes.POINTER(PlanOptions)], i32),
@@ -144,6 +145,17 @@ def _check(status: int, where: str) -> None:
 def secured_log2_length(exponent: int) -> int:
     """NttLengths::GetNttSecuredLength (ntt_lengths.cu:88-98)."""
     return int(lib().lnt_secured_log2_length(exponent))
+
+
+def shifted_words(exponent: int, n: int) -> tuple[int, int]:
+    """(count, first j) of the words where the reference's widths
+    (pre_calculation.cu:35, evaluated in double) start word j one bit below
+    ceil(qj/n), the bit its weight assumes; there the reference's residues are
+    not those of M_q.  This library's widths are the exact integers.  Host only."""
+    count, first = ctypes.c_uint32(), ctypes.c_uint32()
+    _check(lib().lnt_shifted_words(exponent, n, ctypes.byref(count), ctypes.byref(first)),
+           "lnt_shifted_words")
+    return count.value, first.value
 
 
 def length_candidates(exponent: int) -> list[str]:

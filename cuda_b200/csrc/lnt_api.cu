@@ -1034,11 +1034,9 @@ int lnt_create_with_plan(uint32_t exponent, uint32_t n, int prp, int device,
   if (e != cudaSuccess) return bail(cuda_fail(e, "cudaStreamCreate"));
   t->own_stream = true;
 
-  // widths: ceil(q(j+1)/n) - ceil(qj/n) in double, as pre_calculation.cu:35
+  // widths: ceil(q(j+1)/n) - ceil(qj/n), pre_calculation.cu:35 in exact integers
   t->h_widths.resize(n);
-  for (uint32_t j = 0; j < n; ++j)
-    t->h_widths[j] = (uint8_t)(std::ceil(1.0 * exponent * (double)(j + 1) / n) -
-                               std::ceil(1.0 * exponent * (double)j / n));
+  lnt::word_widths(exponent, n, t->h_widths.data());
 
   const uint32_t cb = lnt::canon_block_size(n), nb = n / cb;
   if ((e = dalloc(&t->x, n)) || (e = dalloc(&t->w, n)) || (e = dalloc(&t->uw, n)) ||

@@ -60,6 +60,15 @@ bool make_plan(uint32_t n, uint32_t exponent, const PlanOptions* opt, Plan& plan
 // Every valid explicit plan for (n, q): the autotuner's candidates.
 std::vector<PlanOptions> plan_candidates(uint32_t n, uint32_t exponent);
 
+// Digit widths ceil(q(j+1)/n) - ceil(qj/n) in exact integer arithmetic: word j
+// starts at bit ceil(qj/n), the bit its IBDWT weight 2^(ceil(qj/n) - qj/n) assumes.
+void word_widths(uint32_t exponent, uint32_t n, uint8_t* widths);
+// The words j whose start bit in the reference's table (pre_calculation.cu:35, the
+// same expression in double) is below ceil(qj/n): possible once q*j passes 2^53.
+// Its widths of j - 1 and j are then swapped against these, its weights still
+// assume the exact bit, and its squaring is not that of the number its digits hold.
+std::vector<uint32_t> shifted_words(uint32_t exponent, uint32_t n);
+
 // ------------------------------------------------------------ device ----
 struct DeviceInfo {
   int sms = 0;                   // streaming multiprocessors

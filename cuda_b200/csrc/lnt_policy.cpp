@@ -231,9 +231,37 @@ std::vector<PlanOptions> plan_candidates(uint32_t n, uint32_t exponent) {
   return out;
 }
 
+void word_widths(uint32_t exponent, uint32_t n, uint8_t* widths) {
+  uint64_t start = 0;  // ceil(qj/n)
+  for (uint32_t j = 0; j < n; ++j) {
+    const uint64_t next = ((uint64_t)exponent * (j + 1) + n - 1) / n;
+    widths[j] = (uint8_t)(next - start);
+    start = next;
+  }
+}
+
+std::vector<uint32_t> shifted_words(uint32_t exponent, uint32_t n) {
+  std::vector<uint32_t> out;
+  for (uint32_t j = 1; j < n; ++j) {
+    // the reference's start bit: its double widths telescope to ceil_double(qj/n)
+    const double ref = std::ceil(1.0 * exponent * (double)j / n);
+    if ((uint64_t)ref != ((uint64_t)exponent * j + n - 1) / n) out.push_back(j);
+  }
+  return out;
+}
+
 }  // namespace lnt
 
 extern "C" {
+
+int lnt_shifted_words(uint32_t exponent, uint32_t n, uint32_t* count, uint32_t* first) {
+  if (!count || exponent < 3 || n < 2 || (n & (n - 1)) || n > (1u << lnt::kMaxLog2))
+    return LNT_ERR_INVALID_ARGUMENT;
+  const std::vector<uint32_t> s = lnt::shifted_words(exponent, n);
+  *count = (uint32_t)s.size();
+  if (first) *first = s.empty() ? 0 : s[0];
+  return LNT_OK;
+}
 
 uint32_t lnt_secured_log2_length(uint32_t exponent) { return lnt::secured_log2(exponent); }
 

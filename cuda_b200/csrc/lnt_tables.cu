@@ -4,8 +4,9 @@
 // (calc_brev_factors).  The weights are the same field elements as the
 // reference's: w_j = 7^(((p-1)/192/n) * 5 * (n - r_j)), r_j = q j mod n, w_0 = 1,
 // uw_j = (w_j n)^-1, uw_0 = n^-1.  With g = 7^(((p-1)/192/n) * 5) (g^n = 2),
-// uw_j = g^r_j / (2n) for j > 0.  Widths are computed on the host with the
-// reference's double-precision expression.
+// uw_j = g^r_j / (2n) for j > 0.  The weight of word j thus places it at bit
+// ceil(qj/n) (odd q); the widths (lnt_policy.cpp, word_widths) are the exact
+// integer differences of those bits, so every word starts where its weight says.
 #include "lnt_internal.h"
 #include "goldilocks.cuh"
 

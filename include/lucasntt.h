@@ -11,7 +11,9 @@
  * and never throws; the context owns its device memory.  Digits are the
  * reference's residue words: one uint64 per word, natural order, each word
  * d_j in [0, 2^w_j) with w_j = ceil(q(j+1)/n) - ceil(qj/n), exactly the vector
- * the reference dumps to LucasNTT_results.dat (lucas_prp.cu:254-263).
+ * the reference dumps to LucasNTT_results.dat (lucas_prp.cu:254-263).  The
+ * widths are exact integers; the reference's double-precision table differs from
+ * them only at the words lnt_shifted_words lists (some q at n = 2^25, 2^26).
  */
 #ifndef LUCASNTT_H
 #define LUCASNTT_H
@@ -220,10 +222,22 @@ int lnt_debug_corrupt(lnt_test* t, uint32_t word);
  * raise the kernels' carry flag, which the check also treats as an error. */
 int lnt_debug_corrupt_add(lnt_test* t, uint32_t word, int64_t delta);
 
-/* Length, widths (n bytes, pre_calculation.cu:35) and plan name of a test. */
+/* Length, widths (n bytes: ceil(q(j+1)/n) - ceil(qj/n), pre_calculation.cu:35
+ * in exact integers) and plan name of a test. */
 int lnt_get_length(lnt_test* t, uint32_t* n);
 int lnt_get_widths(lnt_test* t, uint8_t* widths, size_t n);
 int lnt_plan_name(lnt_test* t, char* out, size_t outlen);
+
+/* Words j where the reference's widths differ from this library's.  The
+ * reference evaluates ceil(q(j+1)/n) - ceil(qj/n) in double
+ * (pre_calculation.cu:35); once q*j passes 2^53 (n = 2^25 and 2^26) the double
+ * ceil(qj/n) can land one bit low, so word j starts one bit below the bit its
+ * weight (pre_calculation.cu:30-31) assumes and the reference's squaring is not
+ * that of the number its digits hold: its LL/PRP residues for such (q, n) are not
+ * those of M_q.  This library uses the exact integers (the widths of j - 1 and j
+ * are swapped against the reference's).  *count = how many such j, *first = the
+ * lowest (0 if none; `first` may be NULL).  Host only, no device. */
+int lnt_shifted_words(uint32_t exponent, uint32_t n, uint32_t* count, uint32_t* first);
 
 /* LucasPRP::DumpEnvironment (lucas_prp.cu:265-291): the text of the
  * reference's .env file (CUDA version, devices and their properties). */

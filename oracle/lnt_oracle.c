@@ -301,6 +301,15 @@ void oracle_get_widths(void* p, uint8_t* w) {
     memcpy(w, c->widths, c->n);
 }
 
+/* Replaces the digit widths (the reference's double-precision table) with the
+ * caller's; used to run the same arithmetic on the exact-integer widths
+ * ceil(q(j+1)/n) - ceil(qj/n), which differ from the double ones for some
+ * (q, n) with q*n > 2^53.  Not part of the reference's behaviour. */
+void oracle_set_widths(void* p, const uint8_t* w) {
+    oracle_ctx* c = (oracle_ctx*)p;
+    memcpy(c->widths, w, c->n);
+}
+
 void oracle_get_weights(void* p, uint64_t* w, uint64_t* uw) {
     oracle_ctx* c = (oracle_ctx*)p;
     memcpy(w, c->w, 8ULL * c->n);

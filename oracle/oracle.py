@@ -52,6 +52,7 @@ def lib():
         L.oracle_set_digits.argtypes = [vp, vp]
         L.oracle_get_digits.argtypes = [vp, vp]
         L.oracle_get_widths.argtypes = [vp, vp]
+        L.oracle_set_widths.argtypes = [vp, vp]
         L.oracle_get_weights.argtypes = [vp, vp, vp]
         L.oracle_iterate.argtypes = [vp, u64]
         L.oracle_iterate.restype = ctypes.c_int
@@ -141,6 +142,13 @@ class OracleTest:
         w = np.empty(self.n, np.uint8)
         lib().oracle_get_widths(self._h, w.ctypes.data)
         return w
+
+    def set_widths(self, widths) -> None:
+        """Run on other digit widths (the exact-integer table where the
+        reference's double one differs); not the reference's behaviour."""
+        w = np.ascontiguousarray(widths, dtype=np.uint8)
+        assert w.size == self.n
+        lib().oracle_set_widths(self._h, w.ctypes.data)
 
     def iterate(self, k: int) -> None:
         if lib().oracle_iterate(self._h, int(k)) != 0:

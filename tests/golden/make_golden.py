@@ -120,7 +120,8 @@ def ref_cases() -> list[dict]:
     sampled exponent of each length, and every one of the 256 exponents after
     20,000 squarings.  PRP: full tests of a composite and of Mersenne primes on
     both plan kinds, and q = 139000003 after 1,000 squarings.  C5: full tests of
-    the pool's requests up to q = 610,000."""
+    the pool's requests up to q = 610,000.  Large: 1,000 squarings at 2^24 (LL and
+    PRP), 2^25 and 2^26."""
     from oracle import oracle as O
 
     cases = [{"q": q, "iterations": C4_ITERATIONS, "prp": True, "set": "c4"} for q in c4_exponents()]
@@ -141,6 +142,9 @@ def ref_cases() -> list[dict]:
             seen.add((q, prp))
             cases.append({"q": q, "iterations": q if prp else q - 2, "prp": prp, "set": "c5_full"})
     cases += [{"q": q, "iterations": C3_CHECK_ITERATIONS, "prp": False, "set": "c3_check"} for q in c3_exponents()]
+    # the largest lengths (2^24, 2^25, 2^26: q = 300000007, 600000001, 1100000009), 1,000 squarings
+    cases += [{"q": q, "iterations": 1000, "prp": prp, "set": "large"}
+              for q, prp in ((300000007, False), (300000007, True), (600000001, False), (1100000009, False))]
     return cases
 
 
@@ -158,7 +162,12 @@ def _summaries(dirs: list[str]):
 
 def make_ref(dirs: list[str]) -> None:
     """Merge the reference runs summarised by oracle/run_ref.py (run_*.json:
-    Res64 of the reference's residue dump) into ref_residues.json."""
+    Res64 of the reference's residue dump) into ref_residues.json.  A case whose
+    double-precision widths start some word below its weight's bit carries
+    "shifted_words" (their count): there the reference's sequence is not that of
+    M_q, and true_residues.json holds the true Res64."""
+    from cuda_b200 import shifted_words
+
     path = HERE / "ref_residues.json"
     old = json.loads(path.read_text())["cases"] if path.exists() else []
     key = lambda c: (c["q"], c["n"], c["prp"], c["iterations"])  # noqa: E731
@@ -172,6 +181,10 @@ def make_ref(dirs: list[str]) -> None:
         if (c["q"], c["iterations"], c["prp"]) in sets:
             c["set"] = sets[(c["q"], c["iterations"], c["prp"])]
         merged[key(c)] = c
+    for c in merged.values():
+        k = shifted_words(c["q"], c["n"])[0]
+        if k:
+            c["shifted_words"] = k
     write("ref_residues.json", {
         "source": "reference LucasNTT build (oracle/build_ref.sh) run on a B200 by oracle/run_ref.py; "
                   "Res64 derived from its residue dump; dump_sha256 = SHA-256 of that dump file "

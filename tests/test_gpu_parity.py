@@ -159,14 +159,16 @@ def test_reference_build_residues(lnt):
     10,000 LL squarings and 1,000 PRP squarings at n = 2^23; full PRP tests of
     Mersenne primes (residue 9) and composites on the resident and two-pass
     plans; one C4 exponent per length (PRP, 20,000 squarings); the C3 full LL
-    tests up to 32K words."""
+    tests up to 32K words; 1,000 squarings at 2^24 (LL and PRP) and 2^26.  The
+    2^25 case (q = 600000001) has a shifted word: test_true_residues."""
     cases = _reference_cases()
     c2 = sorted((c for c in cases if c["q"] == 139000003 and not c["prp"]), key=lambda c: c["iterations"])
     c4_lengths = {}
     for c in cases:
         if c.get("set") == "c4":
             c4_lengths.setdefault(c["n"], c)
-    alone_cases = [c for c in cases if c.get("set") in (None, "prp") and c not in c2]
+    alone_cases = [c for c in cases if c.get("set") in (None, "prp", "large") and c not in c2
+                   and not c.get("shifted_words")]
     alone_cases += list(c4_lengths.values())
     alone_cases += [c for c in cases if c.get("set") == "c3_full" and c["n"] <= 32768]
     assert len(c4_lengths) == 3 and sum(c["prp"] for c in alone_cases) >= 9
@@ -183,14 +185,44 @@ def test_reference_build_residues(lnt):
             assert f"{T.res64():016x}" == c["res64"], c
 
 
+def test_true_residues(lnt):
+    """Where the reference's double-precision widths start a word one bit below
+    the bit its weight assumes (q = 600000001 at n = 2^25: j = 23116289), the
+    reference squares another number and its Res64 is not that of M_q.  This
+    library's widths are the exact integers: Res64 equals GMP's big-integer LL
+    sequence (true_residues.json) and differs from the reference build's."""
+    fx = json.loads((GOLDEN / "true_residues.json").read_text())["cases"]
+    ref = {(c["q"], c["n"], c["prp"], c["iterations"]): c["res64"] for c in _reference_cases()}
+    for c in fx:
+        q, n = c["q"], c["n"]
+        count, first = lnt.shifted_words(q, n)
+        assert count > 0
+        with lnt.LucasTest(q, n, c["prp"]) as T:
+            # exact widths; the reference's double table differs at (first - 1, first)
+            j = np.arange(n + 1, dtype=np.uint64)
+            exact = np.diff((np.uint64(q) * j + np.uint64(n - 1)) // np.uint64(n))
+            theirs = np.diff(np.ceil(np.float64(q) * j.astype(np.float64) / n))
+            assert np.array_equal(T.widths(), exact.astype(np.uint8))
+            assert exact[first - 1] != theirs[first - 1] and exact[first] != theirs[first]
+            done = 0
+            for mark in sorted(int(k) for k in c["res64_after"]):
+                T.iterate(mark - done)
+                done = mark
+                got = f"{T.res64():016x}"
+                assert got == c["res64_after"][str(mark)], (c["q"], mark, got)
+                assert got != ref.get((c["q"], c["n"], c["prp"], mark)), "the reference's residue"
+
+
 def test_reference_build_residues_in_one_batch(lnt):
     """Every pinned reference-build residue at once in one batch: resident,
     two-pass and carry-fused plans, LL and PRP mixed -- the nine C1 tests, the
     64 C4 PRP tests (20,000 squarings), the 256 C3 exponents (20,000 LL
     squarings) and one full C3 test per length, the serving stream's full tests
-    up to q = 610,000, the PRP full tests and the C2 exponent (1,000 squarings
-    LL and PRP).  Each Res64 equals the reference build's."""
-    cases = [c for c in _reference_cases() if not (c["q"] == 139000003 and c["iterations"] == 10000)]
+    up to q = 610,000, the PRP full tests, the C2 exponent (1,000 squarings LL
+    and PRP) and 1,000 squarings at 2^24 and 2^26.  Each Res64 equals the
+    reference build's."""
+    cases = [c for c in _reference_cases() if not (c["q"] == 139000003 and c["iterations"] == 10000)
+             and not c.get("shifted_words")]
     want = {}
     with lnt.Batch(device=0) as b:
         for c in cases:

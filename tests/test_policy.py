@@ -1,6 +1,8 @@
 """CPU: the library's length policy equals the reference's (ntt_lengths.cu:32-128)."""
 import random
 
+import numpy as np
+
 import pytest
 
 from oracle import oracle as O
@@ -49,3 +51,37 @@ def test_check_provided_length(lnt):
     assert lnt.check_provided_length(44497, "4096") == -1
     assert lnt.check_provided_length(44497, "1024") == 1
     assert lnt.check_provided_length(139000003, "2048:4096") == 0
+
+
+def _shifted_by_definition(q, n):
+    """Words j > 0 whose start bit (the prefix sum of the double-precision
+    widths of pre_calculation.cu:35) differs from floor(qj/n) + 1, the bit the
+    weight formula of pre_calculation.cu:30-31 assumes."""
+    j = np.arange(n + 1, dtype=np.float64)
+    start = np.ceil(np.float64(q) * j / n)  # = the prefix sums of the widths
+    widths = np.diff(start)
+    assert widths.min() >= q // n and widths.max() <= q // n + 1
+    k = np.arange(1, n, dtype=np.int64)
+    at = (np.int64(q) * k) // n + 1
+    return np.nonzero(start[1:n].astype(np.int64) != at)[0] + 1
+
+
+@pytest.mark.parametrize("q,log2n,count,first", [(600000001, 25, 1, 23116289),
+                                                 (1000000007, 25, 1, 21529527),
+                                                 (300000007, 24, 0, 0), (139000003, 23, 0, 0)])
+def test_shifted_words(lnt, q, log2n, count, first):
+    """Past q*j = 2^53 the double widths start a word one bit below its weight's
+    bit; the library lists exactly the words the definition gives."""
+    want = _shifted_by_definition(q, 1 << log2n)
+    assert lnt.shifted_words(q, 1 << log2n) == (len(want), int(want[0]) if len(want) else 0)
+    assert (len(want), int(want[0]) if len(want) else 0) == (count, first)
+
+
+def test_no_shifted_words_below_2e25(lnt):
+    """q*j < 2^53 for every exponent a length below 2^25 takes (at most 30 bits a
+    word): the double widths are exact there."""
+    for log2n in range(2, 25):
+        n = 1 << log2n
+        q = min(30 * n - 1, 2**31 - 1) | 1
+        assert q * n < 2**53
+        assert lnt.shifted_words(q, n) == (0, 0)
