@@ -18,5 +18,6 @@ from .api import (  # noqa: F401
     plan_describe,
     secured_log2_length,
     shifted_words,
+    smallest_length,
     test_device_bytes,
 )

@@ -85,6 +85,7 @@ def lib() -> ctypes.CDLL:
         "lnt_length_candidates": ([u32, cp, sz], i32),
         "lnt_parse_length": ([cp, ctypes.POINTER(u32)], i32),
         "lnt_check_provided_length": ([u32, cp, ctypes.POINTER(i32)], i32),
+        "lnt_smallest_length": ([u32, ctypes.POINTER(u32)], i32),
         "lnt_shifted_words": ([u32, u32, ctypes.POINTER(u32), ctypes.POINTER(u32)], i32),
         "lnt_create": ([u32, u32, i32, i32, ctypes.POINTER(vp)], i32),
         "lnt_create_with_plan": ([u32, u32, i32, i32, ctypes.POINTER(PlanOptions), ctypes.POINTER(vp)], i32),
@@ -145,6 +146,14 @@ def _check(status: int, where: str) -> None:
 def secured_log2_length(exponent: int) -> int:
     """NttLengths::GetNttSecuredLength (ntt_lengths.cu:88-98)."""
     return int(lib().lnt_secured_log2_length(exponent))
+
+
+def smallest_length(exponent: int) -> int:
+    """lnt_smallest_length: the smallest 2^k or 5 * 2^k length meeting the
+    reference's bound (ntt_lengths.cu:94) that has a plan here."""
+    n = ctypes.c_uint32()
+    _check(lib().lnt_smallest_length(exponent, ctypes.byref(n)), "lnt_smallest_length")
+    return n.value
 
 
 def shifted_words(exponent: int, n: int) -> tuple[int, int]:

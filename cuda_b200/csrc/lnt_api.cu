@@ -48,6 +48,8 @@ struct lnt_test {
   uint64_t *twf = nullptr, *twi = nullptr;
   uint64_t *rt1 = nullptr, *irt1 = nullptr, *rt2 = nullptr, *irt2 = nullptr;
   uint64_t *itw1 = nullptr, *iitw1 = nullptr, *itw2 = nullptr, *iitw2 = nullptr;
+  uint64_t *tw5 = nullptr, *itw5 = nullptr;  // n = 5 * 2^k: the radix-5 step's twiddles
+  uint64_t c5[4] = {};                        // and its constants
   uint64_t *wt = nullptr, *uwt = nullptr;
   uint8_t* widt = nullptr;
   int64_t* carry = nullptr;
@@ -118,7 +120,7 @@ void free_all(lnt_test* t) {
   free_jacobi(t);
   void* ptrs[] = {t->x, t->w, t->uw, t->widths, t->status, t->rt, t->irt, t->rdesc, t->tdesc,
                   t->twf, t->twi, t->rt1, t->irt1, t->rt2, t->irt2, t->itw1, t->iitw1,
-                  t->itw2, t->iitw2, t->wt, t->uwt, t->widt, t->carry, t->fuse, t->canon,
+                  t->itw2, t->iitw2, t->tw5, t->itw5, t->wt, t->uwt, t->widt, t->carry, t->fuse, t->canon,
                   t->blk_carry, t->blk_fn, t->blk_cin, t->cflags};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -224,6 +226,10 @@ lnt::TwoPassDesc twopass_desc(const lnt_test* t) {
   d.ntiles = t->plan.ntiles;
   d.prp = (uint32_t)t->prp;
   d.radix = t->plan.radix;
+  d.five = t->plan.five ? 1 : 0;
+  d.tw5 = t->tw5;
+  d.itw5 = t->itw5;
+  for (int k = 0; k < 4; ++k) d.c5[k] = t->c5[k];
   return d;
 }
 
@@ -433,7 +439,7 @@ int queue_iterations(lnt_test* t, uint64_t iterations, LaunchTimer* timer) {
     d.prp = (uint32_t)t->prp;
     d.unsigned_first = t->canonical_input ? 1 : 0;
     d.iterations = iterations;
-    d.short_runs = lnt::r16_run_words_needed(t->q, t->plan.log2n) <= 4 ? 1 : 0;
+    d.short_runs = lnt::r16_run_words_needed(t->q, t->n) <= 4 ? 1 : 0;
     LNT_CUDA(cudaMemcpyAsync(t->rdesc, &d, sizeof(d), cudaMemcpyHostToDevice, t->stream),
              "upload descriptor");
     LNT_LAUNCH(lnt::launch_resident(t->rdesc, 1, t->n, t->stream), "resident_square_loop");
@@ -929,7 +935,7 @@ ResidentDesc test_resident_desc(const lnt_test* t, uint64_t iterations) {
   d.prp = (uint32_t)t->prp;
   d.unsigned_first = t->canonical_input ? 1 : 0;
   d.iterations = iterations;
-  d.short_runs = r16_run_words_needed(t->q, t->plan.log2n) <= 4 ? 1 : 0;
+  d.short_runs = r16_run_words_needed(t->q, t->n) <= 4 ? 1 : 0;
   return d;
 }
 // bookkeeping after squarings were launched outside lnt_iterate
@@ -1059,7 +1065,13 @@ int lnt_create_with_plan(uint32_t exponent, uint32_t n, int prp, int device,
     if ((st = upload_roots(t, plan.n1, &t->rt1, &t->irt1)) != LNT_OK) return bail(st);
     if ((st = upload_roots(t, plan.n2, &t->rt2, &t->irt2)) != LNT_OK) return bail(st);
     if (plan.fast) {
-      if ((st = upload_roots(t, plan.n1, &t->itw1, &t->iitw1, plan.radix)) != LNT_OK) return bail(st);
+      // pass tables of the row transform: n1 points, or L = n1 / 5 for each plane of a 5 * 2^k row
+      const uint32_t row_points = plan.five ? plan.n1 / 5 : plan.n1;
+      if ((st = upload_roots(t, row_points, &t->itw1, &t->iitw1, plan.radix)) != LNT_OK) return bail(st);
+      if (plan.five &&
+          ((e = dalloc(&t->tw5, 4 * (size_t)row_points)) || (e = dalloc(&t->itw5, 4 * (size_t)row_points)) ||
+           (e = lnt::launch_five_twiddles(row_points, plan.log2n1, t->tw5, t->itw5, t->c5, t->stream))))
+        return bail(cuda_fail(e, "radix-5 twiddles"));
       if ((st = upload_roots(t, plan.n2, &t->itw2, &t->iitw2, plan.radix)) != LNT_OK) return bail(st);
       if ((e = dalloc(&t->wt, n)) || (e = dalloc(&t->uwt, n)) || (e = dalloc(&t->widt, n)) ||
           (e = lnt::launch_tile_major(t->w, t->uw, t->widths, plan.n1, plan.n2, plan.tile, t->wt,
@@ -1079,7 +1091,8 @@ int lnt_create_with_plan(uint32_t exponent, uint32_t n, int prp, int device,
                             hd.irt1, hd.rt2, hd.irt2, hd.status};
     for (const void* ptr : needed)
       if (!ptr) return bail(fail(LNT_ERR_CUDA, "internal: descriptor built before its buffers"));
-    if (plan.fast && (!hd.itw1 || !hd.iitw1 || !hd.itw2 || !hd.iitw2 || !hd.wt || !hd.uwt || !hd.widt))
+    if (plan.fast && (!hd.itw1 || !hd.iitw1 || !hd.itw2 || !hd.iitw2 || !hd.wt || !hd.uwt || !hd.widt ||
+                      (plan.five && (!hd.tw5 || !hd.itw5))))
       return bail(fail(LNT_ERR_CUDA, "internal: descriptor built before its buffers"));
     if ((e = dalloc(&t->tdesc, 1)) ||
         (e = cudaMemcpyAsync(t->tdesc, &hd, sizeof(hd), cudaMemcpyHostToDevice, t->stream)) ||

@@ -502,7 +502,7 @@ int admit(lnt_batch* b, uint64_t id, uint32_t exponent, uint32_t n, int prp, uin
   int st;
   if (b->tune_loops && n > 4096) {
     // one timing per (length, shortest carry run the exponent allows)
-    const uint32_t run = lnt::r16_run_words_needed(exponent, 31 - __builtin_clz(n)) <= 4 ? 4 : 8;
+    const uint32_t run = lnt::r16_run_words_needed(exponent, n) <= 4 ? 4 : 8;
     const uint64_t key = ((uint64_t)n << 8) | run;
     auto it = b->tuned.find(key);
     if (it == b->tuned.end()) {

@@ -36,6 +36,10 @@ struct Plan {
   // the GPU (at n = 2^23: 244.6 us for the pair that takes 270.1 us as two
   // launches); below, where a squaring is latency-bound, two plain launches win
   bool fused = false;
+  // n = 5 * 2^k: rows of n1 = 5 L words, each row transform an L-point NTT of
+  // each of its five stride-5 planes followed by a radix-5 step (register-pass
+  // plans only; log2n1 is then log2 L)
+  bool five = false;
   std::string name;
 };
 
@@ -55,6 +59,8 @@ struct PlanOptions {
 // The plan for an n-word residue of exponent q.  With opt == nullptr (or all
 // zero) the policy chooses; otherwise every non-zero field is honoured or the
 // call fails with the reason in *why.
+// n = 5 * 2^k
+bool five_length(uint32_t n);
 bool make_plan(uint32_t n, uint32_t exponent, const PlanOptions* opt, Plan& plan,
                std::string* why = nullptr);
 // Every valid explicit plan for (n, q): the autotuner's candidates.
@@ -136,6 +142,14 @@ struct TwoPassDesc {
   uint32_t n1, n2, log2n1, log2n2, tile, ntiles;
   uint32_t prp;
   uint32_t radix;  // largest pass radix of the row and column transforms: 8 or 16
+  // n = 5 * 2^k (five != 0): n1 = 5 L and log2n1 = log2 L.  tw5[(j5 - 1) L + e] =
+  // omega_{5L}^(j5 brev_L(e)) for plane j5 = 1..4 and plane position e, itw5 its
+  // inverse; c5 = the radix-5 constants (w + w^4)/2, (w^2 + w^3)/2, (w - w^4)/2,
+  // (w^2 - w^3)/2 of w = omega_5 = omega_{5L}^L
+  uint32_t five;
+  const uint64_t* tw5;
+  const uint64_t* itw5;
+  uint64_t c5[4];
 };
 
 cudaError_t launch_col_forward(const TwoPassDesc& d, bool apply_carries, cudaStream_t s);
@@ -149,7 +163,7 @@ bool r16_supported(uint32_t log2n1, uint32_t log2n2);
 // `radix` (8 or 16) points, first (largest span) first
 std::vector<uint32_t> r16_pass_radices(uint32_t log2L, uint32_t radix);
 uint32_t r16_tile(uint32_t log2n2);
-uint32_t r16_run_words_needed(uint32_t exponent, uint32_t log2n);
+uint32_t r16_run_words_needed(uint32_t exponent, uint32_t n);
 // `d` gives the geometry (shared by every test of the launch); `dd` is a device
 // array of `count` descriptors of tests with that geometry (blockIdx.y picks one).
 cudaError_t launch_col_forward_r16(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
@@ -174,6 +188,10 @@ cudaError_t launch_weights(uint32_t exponent, uint32_t n, uint64_t* w, uint64_t*
                            cudaStream_t s);
 cudaError_t launch_twiddles(uint32_t n1, uint32_t n2, uint32_t log2n2, uint64_t* twf,
                             uint64_t* twi, cudaStream_t s);
+// n = 5 * 2^k rows: the radix-5 step's twiddles for planes of L points (4 L words
+// each) and its constants c5 (TwoPassDesc)
+cudaError_t launch_five_twiddles(uint32_t L, uint32_t log2L, uint64_t* tw5, uint64_t* itw5,
+                                 uint64_t c5[4], cudaStream_t s);
 cudaError_t launch_tile_major(const uint64_t* w, const uint64_t* uw, const uint8_t* widths,
                               uint32_t n1, uint32_t n2, uint32_t tile, uint64_t* wt, uint64_t* uwt,
                               uint8_t* widt, cudaStream_t s);

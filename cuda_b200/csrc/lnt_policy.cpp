@@ -5,6 +5,7 @@
 // bit for bit, including the double-precision arithmetic and the
 // std::to_string(double) spelling of the candidates.  make_plan replaces the
 // autotuned choice among pools (lucas_prp.cu:36-70, kernel_pool.cu:17-142).
+#include <algorithm>
 #include <cctype>
 #include <cmath>
 #include <cstring>
@@ -85,7 +86,8 @@ static void name_plan(Plan& plan) {
     plan.name = "RESIDENT_" + std::to_string(plan.n);
     return;
   }
-  plan.name = "TWOPASS_" + std::to_string(plan.n2) + "x" + std::to_string(plan.n1) +
+  plan.name = "TWOPASS_" + std::to_string(plan.n2) + "x" +
+              (plan.five ? "5x" + std::to_string(plan.n1 / 5) : std::to_string(plan.n1)) +
               (plan.fast ? "_R" + std::to_string(plan.radix) : std::string("_R2")) + "_T" +
               std::to_string(plan.tile) + (plan.fused ? "_F" : "");
 }
@@ -98,6 +100,68 @@ static bool tile_fits(bool fast, uint32_t log2n2, uint32_t tile) {
   return tile == 4 || log2n2 <= 11;
 }
 
+bool five_length(uint32_t n) {
+  return n >= 5 && n % 5 == 0 && ((n / 5) & (n / 5 - 1)) == 0;
+}
+
+// n = 5 * 2^k: register-pass two-pass plans only.  Rows hold n1 = 5 L words (the
+// five stride-5 planes of L words each take the L-point passes, then a radix-5
+// step), columns n2 words as for 2^k; 2^7 <= L <= 2^12, 2^6 <= n2 <= 2^12.
+// Policy: rows of L = 2^11 (87 KB of shared memory) where the columns allow.
+static bool make_five_plan(uint32_t n, uint32_t exponent, PlanOptions o, Plan& plan,
+                           std::string* why) {
+  auto reject = [&](const char* msg) {
+    if (why) *why = msg;
+    return false;
+  };
+  uint32_t k = 0;
+  while ((5u << k) < n) ++k;
+  if (k < 13 || k > 24) return reject("length 5 * 2^k needs 13 <= k <= 24");
+  if (o.kind != 0 && o.kind != 2) return reject("lengths 5 * 2^k run on the register-pass plan only");
+  if (o.radix != 0 && o.radix != 8) return reject("lengths 5 * 2^k take radix-8 passes");
+  if (o.fused > 2) return reject("fused must be 0 (policy), 1 (fused) or 2 (two launches)");
+  plan = Plan();
+  plan.n = n;
+  while ((1ull << plan.log2n) < n) plan.log2n++;
+  plan.kind = PlanKind::TwoPass;
+  plan.fast = true;
+  plan.five = true;
+  uint32_t l2 = o.log2_rows, l1;
+  if (l2 == 0) {
+    l1 = k - 6 < 11 ? k - 6 : 11;
+    l2 = k - l1;
+    if (l2 > 12) {
+      l2 = 12;
+      l1 = k - 12;
+    }
+  } else {
+    if (l2 >= k) return reject("column length exceeds the length");
+    l1 = k - l2;
+  }
+  if (l2 < 6 || l2 > 12 || l1 < 7 || l1 > 12 || (5u << l1) < (1u << l2))
+    return reject("5 * 2^k plan needs 2^6 <= n2 <= 2^12, 2^7 <= L <= 2^12, 5 L >= n2");
+  const uint32_t run_words = exponent ? r16_run_words_needed(exponent, n) : 8;
+  uint32_t tile = o.tile;
+  if (tile == 0) {
+    tile = (run_words <= 4 && tile_fits(true, l2, 4)) ? 4 : 8;
+    if (!tile_fits(true, l2, tile)) tile = 4;
+  } else if (!tile_fits(true, l2, tile)) {
+    return reject("column tile must be 4 or 8 and fit shared memory");
+  } else if (exponent && tile < run_words && tile < 8) {
+    return reject("carry runs of this tile are too short for the exponent");
+  }
+  plan.log2n1 = l1;  // log2 L: the transform length of each plane
+  plan.log2n2 = l2;
+  plan.n1 = 5u << l1;
+  plan.n2 = 1u << l2;
+  plan.tile = tile;
+  plan.ntiles = plan.n1 / tile;
+  plan.radix = 8;
+  plan.fused = o.fused ? o.fused == 1 : plan.log2n >= 19;
+  name_plan(plan);
+  return true;
+}
+
 bool make_plan(uint32_t n, uint32_t exponent, const PlanOptions* opt, Plan& plan,
                std::string* why) {
   auto reject = [&](const char* msg) {
@@ -105,7 +169,9 @@ bool make_plan(uint32_t n, uint32_t exponent, const PlanOptions* opt, Plan& plan
     return false;
   };
   PlanOptions o = opt ? *opt : PlanOptions();
-  if (n < 2 || (n & (n - 1)) || n > (1u << kMaxLog2)) return reject("length must be 2^k, 1 <= k <= 26");
+  if (five_length(n)) return make_five_plan(n, exponent, o, plan, why);
+  if (n < 2 || (n & (n - 1)) || n > (1u << kMaxLog2))
+    return reject("length must be 2^k (1 <= k <= 26) or 5 * 2^k (13 <= k <= 24)");
   if (o.kind > 3) return reject("unknown plan kind");
   if (o.radix != 0 && o.radix != 8 && o.radix != 16) return reject("pass radix must be 8 or 16");
   if (o.fused > 2) return reject("fused must be 0 (policy), 1 (fused) or 2 (two launches)");
@@ -123,7 +189,7 @@ bool make_plan(uint32_t n, uint32_t exponent, const PlanOptions* opt, Plan& plan
   }
   if (plan.log2n <= kResidentMaxLog2) return reject("two-pass plans need n >= 8192");
   plan.kind = PlanKind::TwoPass;
-  const uint32_t run_words = exponent ? r16_run_words_needed(exponent, plan.log2n) : 8;
+  const uint32_t run_words = exponent ? r16_run_words_needed(exponent, n) : 8;
   uint32_t l2 = o.log2_rows, l1;
   if (o.kind == 0) {
     // policy: radix-16 with the most square split the kernels take
@@ -254,6 +320,25 @@ std::vector<uint32_t> shifted_words(uint32_t exponent, uint32_t n) {
 
 extern "C" {
 
+int lnt_smallest_length(uint32_t exponent, uint32_t* n_out) {
+  if (!n_out || exponent < 3) return LNT_ERR_INVALID_ARGUMENT;
+  std::vector<uint32_t> cand;
+  for (uint32_t k = 1; k <= lnt::kMaxLog2; ++k) cand.push_back(1u << k);
+  for (uint32_t k = 13; k <= 24; ++k) cand.push_back(5u << k);
+  std::sort(cand.begin(), cand.end());
+  for (uint32_t n : cand) {
+    if (n > exponent) break;
+    // the reference's bound (ntt_lengths.cu:94): 2 n (2^W - 1)^2 < p, W = ceil(q / n)
+    const double w = std::ceil(1.0 * exponent / n), m = std::exp2(w) - 1;
+    if (w > 30 || m * m >= lnt::kModulus / (2.0 * n)) continue;
+    lnt::Plan plan;
+    if (!lnt::make_plan(n, exponent, nullptr, plan)) continue;
+    *n_out = n;
+    return LNT_OK;
+  }
+  return LNT_ERR_UNSUPPORTED_LENGTH;
+}
+
 int lnt_shifted_words(uint32_t exponent, uint32_t n, uint32_t* count, uint32_t* first) {
   if (!count || exponent < 3 || n < 2 || (n & (n - 1)) || n > (1u << lnt::kMaxLog2))
     return LNT_ERR_INVALID_ARGUMENT;
@@ -285,7 +370,7 @@ int lnt_parse_length(const char* description, uint32_t* n_out) {
   for (auto& f : fs) { n *= f.n; l3 += f.log3; l5 += f.log5; }
   if (n > 0xFFFFFFFFull) return LNT_ERR_INVALID_ARGUMENT;
   *n_out = (uint32_t)n;
-  if (l3 || l5) return LNT_ERR_UNSUPPORTED_LENGTH;
+  if (l3 || l5 > 1) return LNT_ERR_UNSUPPORTED_LENGTH;  // 5 * 2^k has a kernel, 3 * 2^k none
   return LNT_OK;
 }
 

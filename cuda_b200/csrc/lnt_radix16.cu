@@ -231,6 +231,100 @@ __global__ void __launch_bounds__(TH) row_mul_r16(const TwoPassDesc* __restrict_
   }
 }
 
+// ------------------------------------------------------- rows of 5 L ----
+//
+// n = 5 * 2^k: a row holds n1 = 5 L words z[c'], c' = 5 c + j5.  Its transform
+// (root omega_{5L} = omega_n^n2) splits as
+//   Z[kL + L k5] = sum_j5 omega_5^(j5 k5) omega_{5L}^(j5 kL) sum_c z[5 c + j5] omega_L^(c kL):
+// an L-point transform of each stride-5 plane (the passes above, bit-reversed
+// output: plane position e holds kL = brev(e)), a twiddle, and a 5-point
+// transform across the planes at each position.  The radix-5 step is last
+// forward and first inverse, so it runs next to the pointwise square.  The
+// inverse's factor 1/5 is in the unweights (1/n).
+
+// 5-point transform with the pair form: for u1 w^k + u4 w^-k = a1 C + b1 S
+// (a = u1 + u4, b = u1 - u4, C = (w^k + w^-k)/2, S = (w^k - w^-k)/2), eight
+// multiplications instead of sixteen.  c = {C1, C2, S1, S2}.  The inverse
+// transform (w^-1) is the same with outputs 1, 4 and 2, 3 exchanged.
+__device__ __forceinline__ void dft5(uint64_t (&u)[5], const uint64_t* c) {
+  const uint64_t a1 = gl::add(u[1], u[4]), b1 = gl::sub(u[1], u[4]);
+  const uint64_t a2 = gl::add(u[2], u[3]), b2 = gl::sub(u[2], u[3]);
+  const uint64_t t1 = gl::add(gl::mul(a1, c[0]), gl::mul(a2, c[1]));
+  const uint64_t t2 = gl::add(gl::mul(a1, c[1]), gl::mul(a2, c[0]));
+  const uint64_t s1 = gl::add(gl::mul(b1, c[2]), gl::mul(b2, c[3]));
+  const uint64_t s2 = gl::sub(gl::mul(b1, c[3]), gl::mul(b2, c[2]));
+  const uint64_t u0 = u[0];
+  u[0] = gl::add(u0, gl::add(a1, a2));
+  const uint64_t p1 = gl::add(u0, t1), p2 = gl::add(u0, t2);
+  u[1] = gl::add(p1, s1);
+  u[4] = gl::sub(p1, s1);
+  u[2] = gl::add(p2, s2);
+  u[3] = gl::sub(p2, s2);
+}
+
+// Mode 0: square (a squaring), 1: forward only (the operand F of a product,
+// left in x in plane-major order), 2: product with F.
+template <int TH, int MR, int Mode>
+__global__ void __launch_bounds__(TH) row5_r16(const TwoPassDesc* __restrict__ Ds, Passes P,
+                                               const uint64_t* __restrict__ F) {
+  extern __shared__ __align__(16) uint64_t sm[];
+  const TwoPassDesc& D = Ds[blockIdx.y];
+  const int L = (int)D.n1 / 5, ld = padded(L), W = 5 * L;
+  const size_t off = (size_t)blockIdx.x * W;
+  uint64_t* x = reinterpret_cast<uint64_t*>(D.x) + off;
+  // HBM -> planes, with the 4-step twiddle
+  for (int i = threadIdx.x; i < W; i += TH) {
+    const int c = i / 5, j5 = i - 5 * c;
+    sm[j5 * ld + sw(c)] = gl::mul(x[i], D.twf[off + i]);
+  }
+  __syncthreads();
+  int span = L;
+  for (int j = 0, seg = 0; j < P.m; ++j) {
+    pass_r<0, MR>(P.radix[j], sm, ld, 5, L, span, D.itw1 + seg);
+    seg += span;
+    span /= P.radix[j];
+    __syncthreads();
+  }
+  uint64_t c5[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) c5[k] = D.c5[k];
+  for (int e = threadIdx.x; e < L; e += TH) {
+    const int se = sw(e);
+    uint64_t u[5];
+    u[0] = sm[se];
+#pragma unroll
+    for (int j5 = 1; j5 < 5; ++j5) u[j5] = gl::mul(sm[j5 * ld + se], D.tw5[(j5 - 1) * L + e]);
+    dft5(u, c5);
+    if constexpr (Mode == 1) {
+#pragma unroll
+      for (int k5 = 0; k5 < 5; ++k5) x[k5 * L + e] = u[k5];
+      continue;
+    } else {
+#pragma unroll
+      for (int k5 = 0; k5 < 5; ++k5) u[k5] = Mode == 0 ? gl::sqr(u[k5]) : gl::mul(u[k5], F[off + k5 * L + e]);
+      dft5(u, c5);
+      sm[se] = u[0];
+      sm[ld + se] = gl::mul(u[4], D.itw5[e]);
+      sm[2 * ld + se] = gl::mul(u[3], D.itw5[L + e]);
+      sm[3 * ld + se] = gl::mul(u[2], D.itw5[2 * L + e]);
+      sm[4 * ld + se] = gl::mul(u[1], D.itw5[3 * L + e]);
+    }
+  }
+  if constexpr (Mode != 1) {
+    __syncthreads();
+    for (int j = P.m - 1; j >= 0; --j) {
+      span *= P.radix[j];
+      pass_r<1, MR>(P.radix[j], sm, ld, 5, L, span, D.iitw1 + pass_table_offset(P, L, j));
+      __syncthreads();
+    }
+    // planes -> HBM, with the inverse 4-step twiddle
+    for (int i = threadIdx.x; i < W; i += TH) {
+      const int c = i / 5, j5 = i - 5 * c;
+      x[i] = gl::mul(sm[j5 * ld + sw(c)], D.twi[off + i]);
+    }
+  }
+}
+
 // --------------------------------------------------------------- columns ----
 
 // Threads per tile column.  A launch with CTAs enough to fill the GPU
@@ -621,8 +715,9 @@ uint32_t r16_tile(uint32_t log2n2) { return log2n2 >= 12 ? 4 : 8; }
 // Words a carry run needs: the outgoing carry of a run is below 2^(log2 n + W)
 // in magnitude (W = ceil(q / n)), each word it ripples through takes off at
 // least w_min - 1 bits, and the last word absorbs the remaining +-1.
-uint32_t r16_run_words_needed(uint32_t exponent, uint32_t log2n) {
-  const uint32_t n = 1u << log2n;
+uint32_t r16_run_words_needed(uint32_t exponent, uint32_t n) {
+  uint32_t log2n = 0;
+  while ((1ull << log2n) < n) ++log2n;
   const uint32_t wmax = (exponent + n - 1) / n, wmin = exponent / n;
   if (wmin < 3) return 64;
   return (log2n + wmax + wmin - 2) / (wmin - 1) + 1;
@@ -696,17 +791,41 @@ cudaError_t row_square_m(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t c
   }
 }
 
+// One CTA per row of 5 L words (radix-8 passes): 128 threads for up to 1280
+// words, 256 up to 5120, then 512 and 1024.
+template <int Mode>
+cudaError_t row5_launch(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
+                        const uint64_t* F, cudaStream_t s) {
+  const int L = (int)d.n1 / 5;
+  const size_t smem = (size_t)5 * padded(L) * 8;
+  const Passes P = make_passes((int)d.log2n1, 3);
+  const dim3 grid(d.n2, count);
+  auto go = [&](auto kernel, int th) {
+    cudaError_t e = ensure_smem(kernel, smem);
+    if (e != cudaSuccess) return e;
+    kernel<<<grid, th, smem, s>>>(dd, P, F);
+    return cudaGetLastError();
+  };
+  if (d.n1 <= 1280) return go(row5_r16<128, 8, Mode>, 128);
+  if (d.n1 <= 5120) return go(row5_r16<256, 8, Mode>, 256);
+  if (d.n1 <= 10240) return go(row5_r16<512, 8, Mode>, 512);
+  return go(row5_r16<1024, 8, Mode>, 1024);
+}
+
 cudaError_t launch_row_forward_r16(const TwoPassDesc& d, const TwoPassDesc* dd, cudaStream_t s) {
+  if (d.five) return row5_launch<1>(d, dd, 1, nullptr, s);
   return d.radix == 16 ? row_forward_m<16>(d, dd, s) : row_forward_m<8>(d, dd, s);
 }
 
 cudaError_t launch_row_mul_r16(const TwoPassDesc& d, const TwoPassDesc* dd, const uint64_t* F,
                                cudaStream_t s) {
+  if (d.five) return row5_launch<2>(d, dd, 1, F, s);
   return d.radix == 16 ? row_mul_m<16>(d, dd, F, s) : row_mul_m<8>(d, dd, F, s);
 }
 
 cudaError_t launch_row_square_r16(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
                                   cudaStream_t s) {
+  if (d.five) return row5_launch<0>(d, dd, count, nullptr, s);
   return d.radix == 16 ? row_square_m<16>(d, dd, count, s) : row_square_m<8>(d, dd, count, s);
 }
 

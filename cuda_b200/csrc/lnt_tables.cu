@@ -23,7 +23,7 @@ __global__ void weights_kernel(uint32_t exponent, uint32_t n, uint64_t g, uint64
     uw[0] = inv_n;
     return;
   }
-  const uint32_t r = (exponent * j) & (n - 1);  // 32-bit product: only the low bits matter
+  const uint32_t r = (uint32_t)(((uint64_t)exponent * j) % n);
   w[j] = gl::pow(g, (uint64_t)(n - r));
   uw[j] = gl::mul(gl::pow(g, (uint64_t)r), inv_2n);
 }
@@ -73,6 +73,34 @@ cudaError_t launch_weights(uint32_t exponent, uint32_t n, uint64_t* w, uint64_t*
   const uint64_t inv_n = gl::inv(n), inv_2n = gl::inv(2ull * n);
   const uint32_t threads = 256, blocks = (n + threads - 1) / threads;
   weights_kernel<<<blocks, threads, 0, s>>>(exponent, n, g, inv_n, inv_2n, w, uw);
+  return cudaGetLastError();
+}
+
+namespace {
+// tw5[(j5 - 1) L + e] = omega_{5L}^(j5 k), k = brev(e) over log2 L bits: the
+// frequency an L-point plane transform leaves at position e
+__global__ void five_twiddle_kernel(uint32_t L, uint32_t log2L, uint64_t root, uint64_t iroot,
+                                    uint64_t* tw5, uint64_t* itw5) {
+  const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= 4 * L) return;
+  const uint32_t j5 = idx / L + 1, e = idx % L;
+  const uint64_t k = __brev(e) >> (32 - log2L);
+  tw5[idx] = gl::pow(root, j5 * k);
+  itw5[idx] = gl::pow(iroot, j5 * k);
+}
+}  // namespace
+
+cudaError_t launch_five_twiddles(uint32_t L, uint32_t log2L, uint64_t* tw5, uint64_t* itw5,
+                                 uint64_t c5[4], cudaStream_t s) {
+  // omega_{5L} = 554^((p-1)/5L) = omega_n^n2, the same root family as every other table
+  const uint64_t root = gl::pow(554, (gl::P - 1) / (5ull * L)), iroot = gl::inv(root);
+  const uint64_t w = gl::pow(root, L), half = gl::inv(2);  // omega_5
+  const uint64_t w2 = gl::mul(w, w), w3 = gl::mul(w2, w), w4 = gl::mul(w3, w);
+  c5[0] = gl::mul(gl::add(w, w4), half);
+  c5[1] = gl::mul(gl::add(w2, w3), half);
+  c5[2] = gl::mul(gl::sub(w, w4), half);
+  c5[3] = gl::mul(gl::sub(w2, w3), half);
+  five_twiddle_kernel<<<(4 * L + 255) / 256, 256, 0, s>>>(L, log2L, root, iroot, tw5, itw5);
   return cudaGetLastError();
 }
 

@@ -59,8 +59,17 @@ int lnt_length_candidates(uint32_t exponent, char* out, size_t outlen);
  * :130-142): total length of an "fft" description such as "4096", "8M",
  * "2048:4096".  Returns LNT_ERR_INVALID_ARGUMENT for lengths the reference
  * rejects (factors other than 2, 3, 5) and LNT_ERR_UNSUPPORTED_LENGTH for
- * non-power-of-two totals (the reference has no kernel for those either). */
+ * totals other than 2^k and 5 * 2^k (the reference has no kernel for any
+ * non-power-of-two total; this library runs 5 * 2^k, 13 <= k <= 24, on its
+ * register-pass plan, and no IBDWT of length 3 * 2^k exists modulo p). */
 int lnt_parse_length(const char* description, uint32_t* n_out);
+
+/* The smallest length with a plan here that meets the reference's bound
+ * 2n(2^W - 1)^2 < p, W = ceil(q/n) (ntt_lengths.cu:94), among 2^k and 5 * 2^k
+ * (13 <= k <= 24).  Where it is 5 * 2^k it lies between 2^(k+2), which fails
+ * the bound, and the reference's 2^(k+3): 37.5 % fewer words.  Otherwise it is
+ * the power of two the reference picks. */
+int lnt_smallest_length(uint32_t exponent, uint32_t* n_out);
 
 /* NttLengths::CheckProvidedLength (ntt_lengths.cu:77-86): secured log2 length
  * minus log2 of the provided description (> 0: too small, < 0: larger than

@@ -42,12 +42,20 @@ def from_digits(digits, exponent: int, n: int) -> int:
     return v
 
 
+def mod_mersenne(x: int, exponent: int) -> int:
+    """x mod 2^q - 1 for x >= 0 by folding (2^q == 1), no long division."""
+    m = (1 << exponent) - 1
+    while x > m:
+        x = (x & m) + (x >> exponent)
+    return 0 if x == m else x
+
+
 def step(value: int, exponent: int, prp: bool) -> int:
     m = (1 << exponent) - 1
     if value == 0:
         f = 0
     else:
-        f = ((value * value - 1) % m) + 1
+        f = mod_mersenne(value * value - 1, exponent) + 1
     if prp:
         return f
     return f - 2 if f >= 2 else f + m - 2

@@ -1,0 +1,108 @@
+"""GPU: lengths n = 5 * 2^k (rows of five stride-5 planes and a radix-5 step).
+
+The reference has no kernel for any non-power-of-two length, so there is no
+reference residue to pin; the checks are the big-integer model (digit for
+digit), known Mersenne primes, and the length independence of the residue:
+the same test at 5 * 2^k and at a power of two gives the same Res64.
+"""
+import numpy as np
+import pytest
+
+from oracle import bigint_model as B
+
+pytestmark = pytest.mark.gpu
+
+
+def to_digits(v, q, n):
+    """bigint_model.to_digits, vectorised: digit j = bits [pos_j, pos_j + w_j)."""
+    w = np.array(B.widths(q, n), dtype=np.uint64)
+    pos = np.concatenate([[0], np.cumsum(w)[:-1]]).astype(np.uint64)
+    raw = np.frombuffer(v.to_bytes((q + 7) // 8 + 8, "little"), dtype=np.uint8)
+    idx = (pos // np.uint64(8)).astype(np.int64)[:, None] + np.arange(8)
+    words = np.zeros(n, dtype=np.uint64)
+    for b in range(8):
+        words |= raw[idx[:, b]].astype(np.uint64) << np.uint64(8 * b)
+    return (words >> (pos % np.uint64(8))) & ((np.uint64(1) << w) - np.uint64(1))
+
+
+def random_value(q, seed):
+    rng = np.random.default_rng(seed)
+    return int.from_bytes(rng.bytes((q + 7) // 8), "little") % ((1 << q) - 1)
+
+
+@pytest.mark.parametrize("q,n", [(300007, 5 << 13), (1000003, 5 << 15), (4000037, 5 << 17)])
+@pytest.mark.parametrize("prp", [False, True])
+def test_digits_equal_bigint_model(lnt, q, n, prp):
+    """Random canonical state, then 1, 2 and 5 squarings: every digit equal to
+    the model's (exact integer squaring mod M with the reference's carry)."""
+    v = random_value(q, q + n)
+    with lnt.LucasTest(q, n, prp) as T:
+        assert "x5x" in T.plan
+        T.set_digits(to_digits(v, q, n))
+        for k in (1, 2, 5):
+            T.iterate(k)
+            for _ in range(k):
+                v = B.step(v, q, prp)
+            want = to_digits(v, q, n)
+            got = T.digits()
+            bad = np.nonzero(got != want)[0]
+            assert bad.size == 0, (q, n, prp, k, bad[:5])
+            assert T.res64() == B.res64(v)
+
+
+@pytest.mark.parametrize("q,n,prp", [(216091, 5 << 13, False), (216091, 5 << 13, True)])
+def test_known_primes(lnt, q, n, prp):
+    with lnt.LucasTest(q, n, prp) as T:
+        T.iterate(q if prp else q - 2)
+        assert T.is_prime() and T.res64() == (9 if prp else 0)
+
+
+def test_every_plan_of_a_length_agrees(lnt):
+    q, n = 1000003, 5 << 15
+    plans = lnt.plan_candidates(q, n)
+    assert len(plans) > 2
+    got = set()
+    for p in plans:
+        with lnt.LucasTest(q, n, False, plan=p) as T:
+            T.iterate(50)
+            got.add(T.res64())
+    assert len(got) == 1
+
+
+def test_same_residue_as_the_power_of_two_length(lnt):
+    """q = 170000009: the smallest length is 5 * 2^21 (the reference takes 2^24);
+    1,000 squarings give the Res64 of the 2^24 test."""
+    q = 170000009
+    assert lnt.smallest_length(q) == 5 << 21
+    res = []
+    for n in (5 << 21, 1 << 24):
+        with lnt.LucasTest(q, n, False) as T:
+            T.iterate(1000)
+            res.append(T.res64())
+    assert res[0] == res[1]
+
+
+def test_in_a_batch_and_with_the_gerbicz_check(lnt):
+    q, n = 1000003, 5 << 15
+    with lnt.LucasTest(q, n, True) as T:
+        T.iterate(3000)
+        alone = T.res64()
+    with lnt.LucasTest(q, n, True) as T:
+        T.gerbicz_enable(20)  # a check every 400 squarings
+        T.iterate(3000)
+        assert T.res64() == alone
+        st = T.gerbicz_stats()
+        assert st["checks"] >= 7 and st["errors"] == 0
+    with lnt.Batch(device=0) as b:
+        ids = [b.submit(q, n, True, 3000), b.submit(q, 1 << 16, True, 3000), b.submit(300007, 5 << 13, False, 3000)]
+        got = {}
+        for _ in range(100):
+            b.run(1000)
+            for r in b.poll():
+                got[r["id"]] = r
+            if len(got) == len(ids):
+                break
+    assert got[ids[0]]["res64"] == alone and got[ids[1]]["res64"] == alone
+    with lnt.LucasTest(300007, 5 << 13, False) as T:
+        T.iterate(3000)
+        assert got[ids[2]]["res64"] == T.res64()

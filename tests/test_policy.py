@@ -85,3 +85,34 @@ def test_no_shifted_words_below_2e25(lnt):
         q = min(30 * n - 1, 2**31 - 1) | 1
         assert q * n < 2**53
         assert lnt.shifted_words(q, n) == (0, 0)
+
+
+def test_five_lengths(lnt):
+    """5 * 2^k totals parse and have plans (13 <= k <= 24); 3 * 2^k has none."""
+    assert lnt.parse_length("5120") == 5120 and lnt.parse_length("5:2048") == 10240
+    assert "x5x" in lnt.plan_describe(lnt.plan_candidates(300007, 5 << 13)[0], 300007, 5 << 13)
+    for n in (5 << 12, 5 << 25, 3 << 13):
+        with pytest.raises(lnt.LucasNTTError) as e:
+            lnt.plan_candidates(300007 if n < 1e6 else 1000000007, n)
+        assert e.value.status == 2
+    assert all(p[3] == 8 for p in lnt.plan_candidates(1000003, 5 << 15))  # radix-8 passes only
+
+
+def test_smallest_length(lnt):
+    """The smallest 2^k or 5 * 2^k length meeting the reference's bound: never
+    above the reference's power of two, and 5 * 2^k for about a quarter of the
+    exponents (q = 170000009: 5 * 2^21 where the reference takes 2^24)."""
+    rng = random.Random(11)
+    five = 0
+    qs = [rng.randrange(100000, 2**30) for _ in range(500)]
+    for q in qs:
+        n = lnt.smallest_length(q)
+        ref = 1 << O.secured_log2(q)
+        assert n <= ref
+        if n % 5 == 0:
+            five += 1
+            assert n * 8 == ref * 5  # between the failing 2^(k+2) and the reference's 2^(k+3)
+        else:
+            assert n == ref
+    assert 0.1 < five / len(qs) < 0.5
+    assert lnt.smallest_length(170000009) == 5 << 21 and lnt.smallest_length(139000003) == 1 << 23
