@@ -52,7 +52,7 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", choices=["c1", "c2", "c3", "c4", "c5", "lengths"], default="c2",
                     help="c2: one 8M-point LL test (default); c3/c4: batched tests/hour; c5: serving; "
-                         "lengths: one LL test at each of 2^24, 2^25, 2^26")
+                         "lengths: one LL test at each of 2^24, 2^25, 2^26, 5*2^20, 5*2^21")
     ap.add_argument("--seconds", type=float, default=120.0, help="c5: arrival window")
     ap.add_argument("--autotune-loops", type=int, default=20, help="c3/c4: autotuner squarings per candidate (0: policy plans)")
     ap.add_argument("--plan-cache", default="", help="c3/c4: JSON plan cache file")
@@ -244,22 +244,33 @@ def reference_us_per_iteration() -> dict:
 
 
 LENGTH_EXPONENTS = [300000007, 600000001, 1100000009]  # policy lengths 2^24, 2^25, 2^26
+# exponents whose smallest length is 5 * 2^k: 5 * 2^21 (reference 2^24), 5 * 2^20 (2^23)
+FIVE_EXPONENTS = [170000009, 80000023]
+
+
+def length_name(n: int) -> str:
+    return f"2^{n.bit_length() - 1}" if n & (n - 1) == 0 else f"5*2^{(n // 5).bit_length() - 1}"
 
 
 def run_lengths(args):
-    """One LL test alone at each larger policy length: µs per squaring from
-    CUDA events on the test's stream around `--iterations-per-step` squarings
-    (after `--warmup` untimed calls of the same size), the kernel split of one
-    more call, and the reference build's time at that length."""
+    """One LL test alone at each larger policy length, and at the 5 * 2^k
+    lengths of two exponents whose reference length is a power of two 8/5 as
+    long: µs per squaring from CUDA events on the test's stream around
+    `--iterations-per-step` squarings (after `--warmup` untimed calls of the
+    same size), the kernel split of one more call, and the reference build's
+    time at the reference's length for that exponent."""
     import torch
 
     import cuda_b200
 
     ref = reference_us_per_iteration()
     ips = min(args.iterations_per_step, 200)
-    for q in LENGTH_EXPONENTS:
+    cases = [(q, 1 << cuda_b200.secured_log2_length(q)) for q in LENGTH_EXPONENTS]
+    cases += [(q, cuda_b200.smallest_length(q)) for q in FIVE_EXPONENTS]
+    for q, n in cases:
         stream = torch.cuda.Stream()
-        with cuda_b200.LucasTest(q) as t:
+        ref_n = 1 << cuda_b200.secured_log2_length(q)
+        with cuda_b200.LucasTest(q, n) as t:
             t.set_stream(stream.cuda_stream)
             for _ in range(max(args.warmup, 1)):
                 t.iterate(ips)
@@ -271,15 +282,15 @@ def run_lengths(args):
             stream.synchronize()
             us = e0.elapsed_time(e1) * 1e3 / ips
             prof = t.profile_iterations(ips)
-            n = 1 << cuda_b200.secured_log2_length(q)
-            line = {"metric": f"us/iteration, LL q={q} at n=2^{n.bit_length() - 1}", "value": us,
+            line = {"metric": f"us/iteration, LL q={q} at n={length_name(n)}", "value": us,
                     "unit": "us/iteration", "higher_is_better": False, "n_gpus": 1, "dtype": "u64",
                     "data": "LL residue sequence from s0 = 4",
-                    "config": {"workload": f"LL q={q} n=2^{n.bit_length() - 1}", "plan": t.plan,
+                    "config": {"workload": f"LL q={q} n={length_name(n)}", "plan": t.plan,
                                "iterations": ips, "res64": f"{t.res64():016x}"},
                     "kernels": {k: {"launches": v[0], "avg_us": v[1] * 1e3 / max(v[0], 1)}
                                 for k, v in prof.items()},
-                    "reference_build_us_per_iteration": ref.get(n)}
+                    "reference_length": length_name(ref_n),
+                    "reference_build_us_per_iteration": ref.get(ref_n)}
         print(json.dumps(line), flush=True)
 
 

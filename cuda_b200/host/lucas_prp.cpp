@@ -234,7 +234,8 @@ void LucasPRP::DumpStats(double total_ms) {
     r.fft = std::to_string(n2) + ":" + std::to_string(n_ / n2);
     const std::string t = std::to_string(used.tile);
     if (used.kind == LNT_PLAN_RADIX16)
-      r.kernels = {"col_forward_r16<" + t + ">", "row_square_r16", "col_inverse_r16<" + t + ">"};
+      r.kernels = {"col_forward_r16<" + t + ">", n_ % 5 == 0 ? "row5_r16" : "row_square_r16",
+                   "col_inverse_r16<" + t + ">"};
     else
       r.kernels = {"col_forward", "row_square", "col_inverse"};
   } else {

@@ -60,6 +60,9 @@ MainProcess::MainProcess(int argc, char** argv) {
       throw std::runtime_error("Invalid FFT length " + o_.provided_length + ": " + lnt_status_string(st));
     int diff = 0;
     lnt_check_provided_length(o_.exponent, o_.provided_length.c_str(), &diff);
+    uint32_t best = 0;
+    if (n_ % 5 == 0 && lnt_smallest_length(o_.exponent, &best) == LNT_OK)
+      diff = n_ < best ? 1 : (n_ > best ? -1 : 0);  // 5 * 2^k: this library's bound, not log2 alone
     if (diff != 0 &&
         !Confirm(diff > 0 ? "\n\nThe provided length is too small. Due to the risk of overflow, the result will not be reliable.\nDo you still want to process?"
                           : "\n\nThe provided length is not optimal. The process can be accelerated.\nDo you still want to process?"))

@@ -215,3 +215,14 @@ def test_jacobi_check_from_the_ini(tmp_path):
     assert "M(132049) is prime!" in r.stdout
     s = stats(tmp_path / "j.txt")
     assert s["Jacobi checks"] == str((132049 - 2) // 20000) and s["Jacobi errors"] == "0"
+
+
+def test_five_length_from_the_ini(tmp_path):
+    """fft = 40960 (5 * 2^13): no reference kernel has it; the program asks as the
+    reference does for a non-optimal length (this exponent's smallest is 16384),
+    then runs the full LL test of the Mersenne prime M_216091 on it."""
+    r = run_cli(tmp_path, [], ini="Exponent = 216091\nfft = 40960\nPerformanceLoops = 20\n", stdin="y\n")
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "not optimal" in r.stdout and "M(216091) is prime!" in r.stdout
+    s = stats(tmp_path / "LucasNTT_results.txt")
+    assert s["Res64"] == "0000000000000000" and s["fft"] == "64:640"
