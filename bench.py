@@ -245,7 +245,7 @@ def reference_us_per_iteration() -> dict:
 
 LENGTH_EXPONENTS = [300000007, 600000001, 1100000009]  # policy lengths 2^24, 2^25, 2^26
 # exponents whose smallest length is 5 * 2^k: 5 * 2^21 (reference 2^24), 5 * 2^20 (2^23)
-FIVE_EXPONENTS = [170000009, 80000023]
+FIVE_EXPONENTS = [170000009, 100000007]
 
 
 def length_name(n: int) -> str:
