@@ -61,6 +61,9 @@ def parse_args():
     ap.add_argument("--checkpoint-every", type=int, default=20000, help="c3/c4: Res64 checkpoint interval")
     ap.add_argument("--batch-step", type=int, default=2000, help="c3/c4/c5: squarings per engine call")
     ap.add_argument("--c3-count", type=int, default=256, help="c3: tests of the seeded sample to run")
+    ap.add_argument("--short-lengths", action="store_true",
+                    help="c3/c4: the batch runs each test at its smallest length (5*2^k where that "
+                         "meets the bound) instead of the reference's power of two")
     ap.add_argument("--plain", choices=["real", "per-length"], default="per-length",
                     help="c3/c4: plain path run test by test, or summed from per-length times")
     ap.add_argument("--rates", default="0.25,1", help="c5: arrival rates, requests per second")
@@ -413,7 +416,7 @@ def run_batch_workload(args, exps, prp, target_of, label, config, rank=0, world=
             cache = str(Path(tempfile.mkdtemp()) / f"plans_rank{rank}.json")
         tt = time.perf_counter()
         with cuda_b200.Batch(device=local_rank, autotune_loops=args.autotune_loops, plan_cache=cache,
-                             autotune_group=args.autotune_group) as tb:
+                             autotune_group=args.autotune_group, short_lengths=args.short_lengths) as tb:
             for q in mine:
                 tb.submit(q, 0, prp, target_of(q))
         tune_s = time.perf_counter() - tt
@@ -422,7 +425,7 @@ def run_batch_workload(args, exps, prp, target_of, label, config, rank=0, world=
     t0 = time.perf_counter()
     with cuda_b200.Batch(device=local_rank, autotune_loops=args.autotune_loops,
                          plan_cache=cache or None, checkpoint_every=args.checkpoint_every,
-                         autotune_group=args.autotune_group) as b:
+                         autotune_group=args.autotune_group, short_lengths=args.short_lengths) as b:
         ids = {b.submit(q, 0, prp, target_of(q)): q for q in mine}
         t_admitted = time.perf_counter() - t0
         while len(results) < len(ids):
@@ -455,7 +458,7 @@ def run_batch_workload(args, exps, prp, target_of, label, config, rank=0, world=
     if rank == 0:
         lengths = {}
         for q in exps:
-            n = 1 << cuda_b200.secured_log2_length(q)
+            n = cuda_b200.smallest_length(q) if args.short_lengths else 1 << cuda_b200.secured_log2_length(q)
             lengths[n] = lengths.get(n, 0) + 1
         alone = single_test_us(cuda_b200, sorted(exps), prp, local_rank)
         plain_kind = args.plain
@@ -485,6 +488,7 @@ def run_batch_workload(args, exps, prp, target_of, label, config, rank=0, world=
                 "autotune_loops": args.autotune_loops, "autotune_group": args.autotune_group,
                 "tuning_s": tune_s, "tuning": "before the timed run (plans cached in a JSON file)",
                 "plans": plans_used(cache), "lengths": {str(k): v for k, v in sorted(lengths.items())},
+                "short_lengths": args.short_lengths,
                 "plain": plain_kind, "plain_s": plain_s, "plain_tests_per_hour": len(exps) / plain_s * 3600,
                 "speedup_vs_plain": tph / (len(exps) / plain_s * 3600),
                 "alone_us_per_squaring": {str(k): v for k, v in sorted(alone.items())},

@@ -123,6 +123,7 @@ def lib() -> ctypes.CDLL:
         "lnt_debug_corrupt": ([vp, u32], i32),
         "lnt_debug_corrupt_add": ([vp, u32, ctypes.c_int64], i32),
         "lnt_batch_use_graphs": ([vp, i32], i32),
+        "lnt_batch_short_lengths": ([vp, i32], i32),
         "lnt_batch_checkpoint_every": ([vp, u64], i32),
         "lnt_batch_autotune_group": ([vp, u32], i32),
         "lnt_batch_step_seconds": ([vp, ctypes.c_double], i32),
@@ -357,7 +358,7 @@ class Batch:
 
     def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, autotune_loops: int = 0,
                  graphs: bool = True, checkpoint_every: int = 0, plan_cache: str | None = None,
-                 autotune_group: int = 1, step_seconds: float = 0.0):
+                 autotune_group: int = 1, step_seconds: float = 0.0, short_lengths: bool = False):
         h = ctypes.c_void_p()
         _check(lib().lnt_batch_create(device, int(hbm_budget_bytes), ctypes.byref(h)), "lnt_batch_create")
         self._h = h
@@ -373,6 +374,8 @@ class Batch:
             _check(lib().lnt_batch_step_seconds(self._h, float(step_seconds)), "lnt_batch_step_seconds")
         if not graphs:
             _check(lib().lnt_batch_use_graphs(self._h, 0), "lnt_batch_use_graphs")
+        if short_lengths:
+            _check(lib().lnt_batch_short_lengths(self._h, 1), "lnt_batch_short_lengths")
 
     def close(self) -> None:
         if getattr(self, "_h", None):

@@ -959,6 +959,7 @@ uint64_t test_device_bytes(uint32_t n) {
     b += 16ull * n + 8ull * (plan.n1 + plan.n2) + 2ull * n + sizeof(TwoPassDesc) +
          4ull * (plan.n1 + 2);  // fused-kernel flags
     if (plan.fast) b += 16ull * (plan.n1 + plan.n2) + 17ull * n;  // inner twiddles, tile-major tables
+    if (plan.five) b += 64ull * (plan.n1 / 5);                      // radix-5 twiddles
   }
   return b;
 }

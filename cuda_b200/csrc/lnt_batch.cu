@@ -119,6 +119,7 @@ struct lnt_batch {
   cudaEvent_t fork = nullptr;        // recorded on `stream` before the group launches
   cudaEvent_t r0 = nullptr, r1 = nullptr;  // around the resident launch
   bool use_graphs = true;
+  bool short_lengths = false;  // n = 0 requests take lnt_smallest_length (2^k or 5 * 2^k)
   // per-call time budget (lnt_batch_step_seconds; 0: every group advances in lockstep) and the
   // measured seconds per squaring per test of each group geometry, and per word-squaring of
   // the resident launch, that it is split by
@@ -591,8 +592,9 @@ void record_checkpoints(lnt_batch* b) {
   }
 }
 
-int check_request(uint32_t exponent, uint32_t& n) {
-  if (n == 0) n = 1u << lnt_secured_log2_length(exponent);
+int check_request(const lnt_batch* b, uint32_t exponent, uint32_t& n) {
+  if (n == 0 && !(b->short_lengths && lnt_smallest_length(exponent, &n) == LNT_OK))
+    n = 1u << lnt_secured_log2_length(exponent);
   if (lnt::test_device_bytes(n) == 0) return berr(LNT_ERR_UNSUPPORTED_LENGTH, "unsupported length");
   return LNT_OK;
 }
@@ -605,7 +607,7 @@ int lnt_batch_submit(lnt_batch* b, uint32_t exponent, uint32_t n, int prp, uint6
                      uint64_t* id) {
   if (!b) return berr(LNT_ERR_INVALID_ARGUMENT, "null batch");
   DeviceGuard guard(b->device);
-  int st = check_request(exponent, n);
+  int st = check_request(b, exponent, n);
   if (st != LNT_OK) return st;
   if (b->budget && b->used + lnt::test_device_bytes(n) > b->budget)
     return berr(LNT_ERR_BUDGET, "test does not fit the HBM budget");
@@ -619,7 +621,7 @@ int lnt_batch_enqueue(lnt_batch* b, uint32_t exponent, uint32_t n, int prp, uint
                       uint64_t* id) {
   if (!b) return berr(LNT_ERR_INVALID_ARGUMENT, "null batch");
   DeviceGuard guard(b->device);
-  int st = check_request(exponent, n);
+  int st = check_request(b, exponent, n);
   if (st != LNT_OK) return st;
   if (b->budget && lnt::test_device_bytes(n) > b->budget)
     return berr(LNT_ERR_BUDGET, "test larger than the whole HBM budget");
@@ -761,6 +763,12 @@ int lnt_batch_plan_cache(lnt_batch* b, const char* path) {
   if (!b) return berr(LNT_ERR_INVALID_ARGUMENT, "null batch");
   b->cache_path = path ? path : "";
   if (!b->cache_path.empty()) load_plan_cache(b);
+  return LNT_OK;
+}
+
+int lnt_batch_short_lengths(lnt_batch* b, int enable) {
+  if (!b) return berr(LNT_ERR_INVALID_ARGUMENT, "null batch");
+  b->short_lengths = enable != 0;
   return LNT_OK;
 }
 

@@ -361,6 +361,11 @@ int lnt_batch_autotune_group(lnt_batch* b, uint32_t tests);
  * 8 squarings of every group; 0: plain stream launches. */
 int lnt_batch_use_graphs(lnt_batch* b, int enable);
 
+/* enable != 0: requests with n = 0 take lnt_smallest_length (5 * 2^k where that
+ * meets the bound, 37.5 % fewer words) instead of the reference's power of two
+ * (the default).  Residues do not depend on the length. */
+int lnt_batch_short_lengths(lnt_batch* b, int enable);
+
 /* Per-test Res64 checkpoints (no counterpart in the reference, which reports
  * Res64 only at the end of a run, lucas_prp.cu:254-263, so its intermediate
  * residues come from separate runs of k iterations): with every > 0 each test

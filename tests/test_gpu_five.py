@@ -106,3 +106,28 @@ def test_in_a_batch_and_with_the_gerbicz_check(lnt):
     with lnt.LucasTest(300007, 5 << 13, False) as T:
         T.iterate(3000)
         assert got[ids[2]]["res64"] == T.res64()
+
+
+def test_short_length_batch_matches_reference_pins(lnt):
+    """A batch with short lengths on runs the C4 exponents whose smallest length is
+    5 * 2^k (327,680 or 655,360 words instead of the reference's 2^19 / 2^20) and
+    gives the reference build's Res64 after 20,000 PRP squarings."""
+    import json
+    from pathlib import Path
+
+    cases = json.loads((Path(__file__).resolve().parent / "golden" / "ref_residues.json").read_text())["cases"]
+    c4 = [c for c in cases if c.get("set") == "c4" and lnt.smallest_length(c["q"]) % 5 == 0][:8]
+    assert len(c4) == 8
+    with lnt.Batch(device=0, short_lengths=True) as b:
+        want = {b.submit(c["q"], 0, True, c["iterations"]): c for c in c4}
+        got = {}
+        for _ in range(200):
+            b.run(4000)
+            for r in b.poll():
+                got[r["id"]] = r
+            if len(got) == len(want):
+                break
+    assert set(got) == set(want)
+    for i, r in got.items():
+        assert r["n"] == lnt.smallest_length(want[i]["q"]) < want[i]["n"]
+        assert r["status"] == 0 and f"{r['res64']:016x}" == want[i]["res64"], want[i]
