@@ -263,24 +263,25 @@ __device__ __forceinline__ void dft5(uint64_t (&u)[5], const uint64_t* c) {
 }
 
 // Mode 0: square (a squaring), 1: forward only (the operand F of a product,
-// left in x in plane-major order), 2: product with F.
+// left in x in plane-major order), 2: product with F.  A CTA takes `rows`
+// consecutive rows (5 rows planes, plane 5 g + j5 at sm + (5 g + j5) ld).
 template <int TH, int MR, int Mode>
-__global__ void __launch_bounds__(TH) row5_r16(const TwoPassDesc* __restrict__ Ds, Passes P,
+__global__ void __launch_bounds__(TH) row5_r16(const TwoPassDesc* __restrict__ Ds, Passes P, int rows,
                                                const uint64_t* __restrict__ F) {
   extern __shared__ __align__(16) uint64_t sm[];
   const TwoPassDesc& D = Ds[blockIdx.y];
-  const int L = (int)D.n1 / 5, ld = padded(L), W = 5 * L;
-  const size_t off = (size_t)blockIdx.x * W;
+  const int L = (int)D.n1 / 5, ld = padded(L), W = 5 * L, lL = __ffs(L) - 1;
+  const size_t off = (size_t)blockIdx.x * rows * W;
   uint64_t* x = reinterpret_cast<uint64_t*>(D.x) + off;
   // HBM -> planes, with the 4-step twiddle
-  for (int i = threadIdx.x; i < W; i += TH) {
-    const int c = i / 5, j5 = i - 5 * c;
-    sm[j5 * ld + sw(c)] = gl::mul(x[i], D.twf[off + i]);
+  for (int i = threadIdx.x; i < rows * W; i += TH) {
+    const int g = i / W, cc = i - g * W, c = cc / 5, j5 = cc - 5 * c;
+    sm[(5 * g + j5) * ld + sw(c)] = gl::mul(x[i], D.twf[off + i]);
   }
   __syncthreads();
   int span = L;
   for (int j = 0, seg = 0; j < P.m; ++j) {
-    pass_r<0, MR>(P.radix[j], sm, ld, 5, L, span, D.itw1 + seg);
+    pass_r<0, MR>(P.radix[j], sm, ld, 5 * rows, L, span, D.itw1 + seg);
     seg += span;
     span /= P.radix[j];
     __syncthreads();
@@ -288,39 +289,41 @@ __global__ void __launch_bounds__(TH) row5_r16(const TwoPassDesc* __restrict__ D
   uint64_t c5[4];
 #pragma unroll
   for (int k = 0; k < 4; ++k) c5[k] = D.c5[k];
-  for (int e = threadIdx.x; e < L; e += TH) {
-    const int se = sw(e);
+  for (int item = threadIdx.x; item < rows * L; item += TH) {
+    const int g = item >> lL, e = item & (L - 1);
+    uint64_t* base = sm + 5 * g * ld + sw(e);
     uint64_t u[5];
-    u[0] = sm[se];
+    u[0] = base[0];
 #pragma unroll
-    for (int j5 = 1; j5 < 5; ++j5) u[j5] = gl::mul(sm[j5 * ld + se], D.tw5[(j5 - 1) * L + e]);
+    for (int j5 = 1; j5 < 5; ++j5) u[j5] = gl::mul(base[j5 * ld], D.tw5[(j5 - 1) * L + e]);
     dft5(u, c5);
     if constexpr (Mode == 1) {
 #pragma unroll
-      for (int k5 = 0; k5 < 5; ++k5) x[k5 * L + e] = u[k5];
+      for (int k5 = 0; k5 < 5; ++k5) x[g * W + k5 * L + e] = u[k5];
       continue;
     } else {
 #pragma unroll
-      for (int k5 = 0; k5 < 5; ++k5) u[k5] = Mode == 0 ? gl::sqr(u[k5]) : gl::mul(u[k5], F[off + k5 * L + e]);
+      for (int k5 = 0; k5 < 5; ++k5)
+        u[k5] = Mode == 0 ? gl::sqr(u[k5]) : gl::mul(u[k5], F[off + g * W + k5 * L + e]);
       dft5(u, c5);
-      sm[se] = u[0];
-      sm[ld + se] = gl::mul(u[4], D.itw5[e]);
-      sm[2 * ld + se] = gl::mul(u[3], D.itw5[L + e]);
-      sm[3 * ld + se] = gl::mul(u[2], D.itw5[2 * L + e]);
-      sm[4 * ld + se] = gl::mul(u[1], D.itw5[3 * L + e]);
+      base[0] = u[0];
+      base[ld] = gl::mul(u[4], D.itw5[e]);
+      base[2 * ld] = gl::mul(u[3], D.itw5[L + e]);
+      base[3 * ld] = gl::mul(u[2], D.itw5[2 * L + e]);
+      base[4 * ld] = gl::mul(u[1], D.itw5[3 * L + e]);
     }
   }
   if constexpr (Mode != 1) {
     __syncthreads();
     for (int j = P.m - 1; j >= 0; --j) {
       span *= P.radix[j];
-      pass_r<1, MR>(P.radix[j], sm, ld, 5, L, span, D.iitw1 + pass_table_offset(P, L, j));
+      pass_r<1, MR>(P.radix[j], sm, ld, 5 * rows, L, span, D.iitw1 + pass_table_offset(P, L, j));
       __syncthreads();
     }
     // planes -> HBM, with the inverse 4-step twiddle
-    for (int i = threadIdx.x; i < W; i += TH) {
-      const int c = i / 5, j5 = i - 5 * c;
-      x[i] = gl::mul(sm[j5 * ld + sw(c)], D.twi[off + i]);
+    for (int i = threadIdx.x; i < rows * W; i += TH) {
+      const int g = i / W, cc = i - g * W, c = cc / 5, j5 = cc - 5 * c;
+      x[i] = gl::mul(sm[(5 * g + j5) * ld + sw(c)], D.twi[off + i]);
     }
   }
 }
@@ -791,24 +794,31 @@ cudaError_t row_square_m(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t c
   }
 }
 
-// One CTA per row of 5 L words (radix-8 passes): 128 threads for up to 1280
-// words, 256 up to 5120, then 512 and 1024.
+// Rows of 5 L words (radix-8 passes) per CTA: as many as fit 4096 words (a
+// power of two), fewer while the launch would have fewer CTAs than the SMs (one
+// test) or than four per SM (a batch of `count`); 128 threads for up to 1280
+// words a CTA, 256 up to 5120, then 512 and 1024.
 template <int Mode>
 cudaError_t row5_launch(const TwoPassDesc& d, const TwoPassDesc* dd, uint32_t count,
                         const uint64_t* F, cudaStream_t s) {
   const int L = (int)d.n1 / 5;
-  const size_t smem = (size_t)5 * padded(L) * 8;
+  int rows = 1;
+  while (rows * 2 * (int)d.n1 <= 4096 && rows * 2 <= (int)d.n2) rows *= 2;
+  const long want = count > 1 ? 4L * device_sms() : (long)device_sms();
+  while (rows > 1 && (long)(d.n2 / rows) * (long)count < want) rows /= 2;
+  const size_t smem = (size_t)5 * rows * padded(L) * 8;
   const Passes P = make_passes((int)d.log2n1, 3);
-  const dim3 grid(d.n2, count);
+  const dim3 grid(d.n2 / rows, count);
+  const int words = rows * (int)d.n1;
   auto go = [&](auto kernel, int th) {
     cudaError_t e = ensure_smem(kernel, smem);
     if (e != cudaSuccess) return e;
-    kernel<<<grid, th, smem, s>>>(dd, P, F);
+    kernel<<<grid, th, smem, s>>>(dd, P, rows, F);
     return cudaGetLastError();
   };
-  if (d.n1 <= 1280) return go(row5_r16<128, 8, Mode>, 128);
-  if (d.n1 <= 5120) return go(row5_r16<256, 8, Mode>, 256);
-  if (d.n1 <= 10240) return go(row5_r16<512, 8, Mode>, 512);
+  if (words <= 1280) return go(row5_r16<128, 8, Mode>, 128);
+  if (words <= 5120) return go(row5_r16<256, 8, Mode>, 256);
+  if (words <= 10240) return go(row5_r16<512, 8, Mode>, 512);
   return go(row5_r16<1024, 8, Mode>, 1024);
 }
 

@@ -131,3 +131,28 @@ def test_short_length_batch_matches_reference_pins(lnt):
     for i, r in got.items():
         assert r["n"] == lnt.smallest_length(want[i]["q"]) < want[i]["n"]
         assert r["status"] == 0 and f"{r['res64']:016x}" == want[i]["res64"], want[i]
+
+
+def test_batched_rows_per_cta(lnt, tmp_path):
+    """Twelve tests of one 5 * 2^15 plan with rows of 640 words (forced through a
+    plan cache) run as one launch group whose row kernel packs four rows per CTA;
+    every residue equals the test alone (one row per CTA, the policy's plan)."""
+    import json
+
+    import torch
+
+    n = 5 << 15
+    cache = tmp_path / "plans.json"
+    cache.write_text(json.dumps({"device": torch.cuda.get_device_name(0), "plans": [
+        {"n": n, "run": 8, "kind": 2, "log2_rows": 8, "tile": 8, "radix": 8, "fused": 2, "ms": 1}]}))
+    qs = [1000003 + 2 * i for i in range(12)]
+    with lnt.Batch(device=0, autotune_loops=5, plan_cache=str(cache)) as b:
+        ids = {b.submit(q, n, False, 30): q for q in qs}
+        got = {}
+        while len(got) < len(ids):
+            b.run(30)
+            got.update({r["id"]: r for r in b.poll()})
+    for i, q in ids.items():
+        with lnt.LucasTest(q, n, False) as T:
+            T.iterate(30)
+            assert got[i]["status"] == 0 and got[i]["res64"] == T.res64(), q
