@@ -8,7 +8,7 @@ own residues are not those of M_q.  Independent of this package and of the
 oracle: s <- s^2 (- 2 for LL) mod 2^q - 1 with mpz_mul and a shift-and-add
 reduction.
 
-    python tests/golden/make_true_residues.py            # about 70 min
+    python tests/golden/make_true_residues.py            # about an hour
 """
 import ctypes
 import ctypes.util
