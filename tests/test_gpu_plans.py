@@ -22,7 +22,12 @@ def random_digits(q, n, seed):
 
 
 def oracle_digits(oracle_mod, q, n, prp, start, steps):
+    """The oracle on the exact integer widths the library uses: they differ from
+    the reference's double ones only where those break the squaring (q = 600000001
+    at 2^25), and there the oracle then squares the number the digits hold."""
     with oracle_mod.OracleTest(q, n, prp) as O:
+        j = np.arange(n + 1, dtype=np.uint64)
+        O.set_widths(np.diff((np.uint64(q) * j + np.uint64(n - 1)) // np.uint64(n)).astype(np.uint8))
         O.set_digits(start)
         O.iterate(steps)
         return O.digits()
