@@ -1071,7 +1071,7 @@ int lnt_create_with_plan(uint32_t exponent, uint32_t n, int prp, int device,
       if ((st = upload_roots(t, row_points, &t->itw1, &t->iitw1, plan.radix)) != LNT_OK) return bail(st);
       if (plan.five &&
           ((e = dalloc(&t->tw5, 4 * (size_t)row_points)) || (e = dalloc(&t->itw5, 4 * (size_t)row_points)) ||
-           (e = lnt::launch_five_twiddles(row_points, plan.log2n1, t->tw5, t->itw5, t->c5, t->stream))))
+           (e = lnt::launch_five_twiddles(row_points, t->tw5, t->itw5, t->c5, t->stream))))
         return bail(cuda_fail(e, "radix-5 twiddles"));
       if ((st = upload_roots(t, plan.n2, &t->itw2, &t->iitw2, plan.radix)) != LNT_OK) return bail(st);
       if ((e = dalloc(&t->wt, n)) || (e = dalloc(&t->uwt, n)) || (e = dalloc(&t->widt, n)) ||

@@ -36,9 +36,9 @@ struct Plan {
   // the GPU (at n = 2^23: 244.6 us for the pair that takes 270.1 us as two
   // launches); below, where a squaring is latency-bound, two plain launches win
   bool fused = false;
-  // n = 5 * 2^k: rows of n1 = 5 L words, each row transform an L-point NTT of
-  // each of its five stride-5 planes followed by a radix-5 step (register-pass
-  // plans only; log2n1 is then log2 L)
+  // n = 5 * 2^k: rows of n1 = 5 L words, each row transform a radix-5 step over
+  // the words c + L j5 followed by an L-point NTT of each of the five planes
+  // (register-pass plans only; log2n1 is then log2 L)
   bool five = false;
   std::string name;
 };
@@ -142,8 +142,8 @@ struct TwoPassDesc {
   uint32_t n1, n2, log2n1, log2n2, tile, ntiles;
   uint32_t prp;
   uint32_t radix;  // largest pass radix of the row and column transforms: 8 or 16
-  // n = 5 * 2^k (five != 0): n1 = 5 L and log2n1 = log2 L.  tw5[(j5 - 1) L + e] =
-  // omega_{5L}^(j5 brev_L(e)) for plane j5 = 1..4 and plane position e, itw5 its
+  // n = 5 * 2^k (five != 0): n1 = 5 L and log2n1 = log2 L.  tw5[(k5 - 1) L + c] =
+  // omega_{5L}^(k5 c) for plane k5 = 1..4 and plane position c, itw5 its
   // inverse; c5 = the radix-5 constants (w + w^4)/2, (w^2 + w^3)/2, (w - w^4)/2,
   // (w^2 - w^3)/2 of w = omega_5 = omega_{5L}^L
   uint32_t five;
@@ -190,8 +190,8 @@ cudaError_t launch_twiddles(uint32_t n1, uint32_t n2, uint32_t log2n2, uint64_t*
                             uint64_t* twi, cudaStream_t s);
 // n = 5 * 2^k rows: the radix-5 step's twiddles for planes of L points (4 L words
 // each) and its constants c5 (TwoPassDesc)
-cudaError_t launch_five_twiddles(uint32_t L, uint32_t log2L, uint64_t* tw5, uint64_t* itw5,
-                                 uint64_t c5[4], cudaStream_t s);
+cudaError_t launch_five_twiddles(uint32_t L, uint64_t* tw5, uint64_t* itw5, uint64_t c5[4],
+                                 cudaStream_t s);
 cudaError_t launch_tile_major(const uint64_t* w, const uint64_t* uw, const uint8_t* widths,
                               uint32_t n1, uint32_t n2, uint32_t tile, uint64_t* wt, uint64_t* uwt,
                               uint8_t* widt, cudaStream_t s);

@@ -233,14 +233,14 @@ __global__ void __launch_bounds__(TH) row_mul_r16(const TwoPassDesc* __restrict_
 
 // ------------------------------------------------------- rows of 5 L ----
 //
-// n = 5 * 2^k: a row holds n1 = 5 L words z[c'], c' = 5 c + j5.  Its transform
+// n = 5 * 2^k: a row holds n1 = 5 L words z[c'], c' = c + L j5.  Its transform
 // (root omega_{5L} = omega_n^n2) splits as
-//   Z[kL + L k5] = sum_j5 omega_5^(j5 k5) omega_{5L}^(j5 kL) sum_c z[5 c + j5] omega_L^(c kL):
-// an L-point transform of each stride-5 plane (the passes above, bit-reversed
-// output: plane position e holds kL = brev(e)), a twiddle, and a 5-point
-// transform across the planes at each position.  The radix-5 step is last
-// forward and first inverse, so it runs next to the pointwise square.  The
-// inverse's factor 1/5 is in the unweights (1/n).
+//   Z[5 kL + k5] = sum_c omega_L^(c kL) omega_{5L}^(c k5) sum_j5 omega_5^(j5 k5) z[c + L j5]:
+// a 5-point transform of the five words c, c + L, ..., c + 4L (fused with the
+// 4-step twiddle as the row is loaded), a twiddle, and an L-point transform of
+// each of the five planes (the passes above, bit-reversed output), whose last
+// pass runs with the square as in row_square_r16.  The inverse runs the same
+// steps backwards and stores the row; its factor 1/5 is in the unweights (1/n).
 
 // 5-point transform with the pair form: for u1 w^k + u4 w^-k = a1 C + b1 S
 // (a = u1 + u4, b = u1 - u4, C = (w^k + w^-k)/2, S = (w^k - w^-k)/2), eight
@@ -264,7 +264,7 @@ __device__ __forceinline__ void dft5(uint64_t (&u)[5], const uint64_t* c) {
 
 // Mode 0: square (a squaring), 1: forward only (the operand F of a product,
 // left in x in plane-major order), 2: product with F.  A CTA takes `rows`
-// consecutive rows (5 rows planes, plane 5 g + j5 at sm + (5 g + j5) ld).
+// consecutive rows: plane k5 of row g at sm + (5 g + k5) ld.
 template <int TH, int MR, int Mode>
 __global__ void __launch_bounds__(TH) row5_r16(const TwoPassDesc* __restrict__ Ds, Passes P, int rows,
                                                const uint64_t* __restrict__ F) {
@@ -273,57 +273,65 @@ __global__ void __launch_bounds__(TH) row5_r16(const TwoPassDesc* __restrict__ D
   const int L = (int)D.n1 / 5, ld = padded(L), W = 5 * L, lL = __ffs(L) - 1;
   const size_t off = (size_t)blockIdx.x * rows * W;
   uint64_t* x = reinterpret_cast<uint64_t*>(D.x) + off;
-  // HBM -> planes, with the 4-step twiddle
-  for (int i = threadIdx.x; i < rows * W; i += TH) {
-    const int g = i / W, cc = i - g * W, c = cc / 5, j5 = cc - 5 * c;
-    sm[(5 * g + j5) * ld + sw(c)] = gl::mul(x[i], D.twf[off + i]);
+  const uint64_t* twf = D.twf + off;
+  uint64_t c5[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) c5[k] = D.c5[k];
+  // HBM -> planes: 4-step twiddle, 5-point transform, twiddle omega_5L^(c k5)
+  for (int item = threadIdx.x; item < rows * L; item += TH) {
+    const int g = item >> lL, c = item & (L - 1);
+    const int i0 = g * W + c;
+    uint64_t u[5];
+#pragma unroll
+    for (int j5 = 0; j5 < 5; ++j5) u[j5] = gl::mul(x[i0 + j5 * L], twf[i0 + j5 * L]);
+    dft5(u, c5);
+    uint64_t* base = sm + 5 * g * ld + sw(c);
+    base[0] = u[0];
+#pragma unroll
+    for (int k5 = 1; k5 < 5; ++k5) base[k5 * ld] = gl::mul(u[k5], D.tw5[(k5 - 1) * L + c]);
   }
   __syncthreads();
   int span = L;
-  for (int j = 0, seg = 0; j < P.m; ++j) {
+  const int last = Mode == 1 ? P.m : P.m - 1;
+  for (int j = 0, seg = 0; j < last; ++j) {
     pass_r<0, MR>(P.radix[j], sm, ld, 5 * rows, L, span, D.itw1 + seg);
     seg += span;
     span /= P.radix[j];
     __syncthreads();
   }
-  uint64_t c5[4];
-#pragma unroll
-  for (int k = 0; k < 4; ++k) c5[k] = D.c5[k];
-  for (int item = threadIdx.x; item < rows * L; item += TH) {
-    const int g = item >> lL, e = item & (L - 1);
-    uint64_t* base = sm + 5 * g * ld + sw(e);
-    uint64_t u[5];
-    u[0] = base[0];
-#pragma unroll
-    for (int j5 = 1; j5 < 5; ++j5) u[j5] = gl::mul(base[j5 * ld], D.tw5[(j5 - 1) * L + e]);
-    dft5(u, c5);
-    if constexpr (Mode == 1) {
-#pragma unroll
-      for (int k5 = 0; k5 < 5; ++k5) x[g * W + k5 * L + e] = u[k5];
-      continue;
-    } else {
-#pragma unroll
-      for (int k5 = 0; k5 < 5; ++k5)
-        u[k5] = Mode == 0 ? gl::sqr(u[k5]) : gl::mul(u[k5], F[off + g * W + k5 * L + e]);
-      dft5(u, c5);
-      base[0] = u[0];
-      base[ld] = gl::mul(u[4], D.itw5[e]);
-      base[2 * ld] = gl::mul(u[3], D.itw5[L + e]);
-      base[3 * ld] = gl::mul(u[2], D.itw5[2 * L + e]);
-      base[4 * ld] = gl::mul(u[1], D.itw5[3 * L + e]);
+  if constexpr (Mode == 1) {
+    for (int i = threadIdx.x; i < rows * W; i += TH) {
+      const int p = i >> lL, e = i & (L - 1);
+      x[i] = sm[p * ld + sw(e)];
     }
-  }
-  if constexpr (Mode != 1) {
+  } else {
+    // last forward pass, square (or product with F) and first inverse pass
+    if constexpr (Mode == 0)
+      pass_r<2, MR>(P.radix[P.m - 1], sm, ld, 5 * rows, L, span, nullptr);
+    else
+      pass_r<3, MR>(P.radix[P.m - 1], sm, ld, 5 * rows, L, span, F + off);
     __syncthreads();
-    for (int j = P.m - 1; j >= 0; --j) {
+    for (int j = P.m - 2; j >= 0; --j) {
       span *= P.radix[j];
       pass_r<1, MR>(P.radix[j], sm, ld, 5 * rows, L, span, D.iitw1 + pass_table_offset(P, L, j));
       __syncthreads();
     }
-    // planes -> HBM, with the inverse 4-step twiddle
-    for (int i = threadIdx.x; i < rows * W; i += TH) {
-      const int g = i / W, cc = i - g * W, c = cc / 5, j5 = cc - 5 * c;
-      x[i] = gl::mul(sm[(5 * g + j5) * ld + sw(c)], D.twi[off + i]);
+    // planes -> HBM: inverse twiddle, inverse 5-point transform, inverse 4-step twiddle
+    const uint64_t* twi = D.twi + off;
+    for (int item = threadIdx.x; item < rows * L; item += TH) {
+      const int g = item >> lL, c = item & (L - 1);
+      const int i0 = g * W + c;
+      const uint64_t* base = sm + 5 * g * ld + sw(c);
+      uint64_t u[5];
+      u[0] = base[0];
+#pragma unroll
+      for (int k5 = 1; k5 < 5; ++k5) u[k5] = gl::mul(base[k5 * ld], D.itw5[(k5 - 1) * L + c]);
+      dft5(u, c5);
+      x[i0] = gl::mul(u[0], twi[i0]);
+      x[i0 + L] = gl::mul(u[4], twi[i0 + L]);
+      x[i0 + 2 * L] = gl::mul(u[3], twi[i0 + 2 * L]);
+      x[i0 + 3 * L] = gl::mul(u[2], twi[i0 + 3 * L]);
+      x[i0 + 4 * L] = gl::mul(u[1], twi[i0 + 4 * L]);
     }
   }
 }

@@ -77,21 +77,20 @@ cudaError_t launch_weights(uint32_t exponent, uint32_t n, uint64_t* w, uint64_t*
 }
 
 namespace {
-// tw5[(j5 - 1) L + e] = omega_{5L}^(j5 k), k = brev(e) over log2 L bits: the
-// frequency an L-point plane transform leaves at position e
-__global__ void five_twiddle_kernel(uint32_t L, uint32_t log2L, uint64_t root, uint64_t iroot,
-                                    uint64_t* tw5, uint64_t* itw5) {
+// tw5[(k5 - 1) L + c] = omega_{5L}^(k5 c): the twiddle between the 5-point
+// transform of the words c + L j5 and the L-point transform of plane k5
+__global__ void five_twiddle_kernel(uint32_t L, uint64_t root, uint64_t iroot, uint64_t* tw5,
+                                    uint64_t* itw5) {
   const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= 4 * L) return;
-  const uint32_t j5 = idx / L + 1, e = idx % L;
-  const uint64_t k = __brev(e) >> (32 - log2L);
-  tw5[idx] = gl::pow(root, j5 * k);
-  itw5[idx] = gl::pow(iroot, j5 * k);
+  const uint64_t e = (uint64_t)(idx / L + 1) * (idx % L);
+  tw5[idx] = gl::pow(root, e);
+  itw5[idx] = gl::pow(iroot, e);
 }
 }  // namespace
 
-cudaError_t launch_five_twiddles(uint32_t L, uint32_t log2L, uint64_t* tw5, uint64_t* itw5,
-                                 uint64_t c5[4], cudaStream_t s) {
+cudaError_t launch_five_twiddles(uint32_t L, uint64_t* tw5, uint64_t* itw5, uint64_t c5[4],
+                                 cudaStream_t s) {
   // omega_{5L} = 554^((p-1)/5L) = omega_n^n2, the same root family as every other table
   const uint64_t root = gl::pow(554, (gl::P - 1) / (5ull * L)), iroot = gl::inv(root);
   const uint64_t w = gl::pow(root, L), half = gl::inv(2);  // omega_5
@@ -100,7 +99,7 @@ cudaError_t launch_five_twiddles(uint32_t L, uint32_t log2L, uint64_t* tw5, uint
   c5[1] = gl::mul(gl::add(w2, w3), half);
   c5[2] = gl::mul(gl::sub(w, w4), half);
   c5[3] = gl::mul(gl::sub(w2, w3), half);
-  five_twiddle_kernel<<<(4 * L + 255) / 256, 256, 0, s>>>(L, log2L, root, iroot, tw5, itw5);
+  five_twiddle_kernel<<<(4 * L + 255) / 256, 256, 0, s>>>(L, root, iroot, tw5, itw5);
   return cudaGetLastError();
 }
 

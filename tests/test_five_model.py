@@ -3,12 +3,13 @@
 A model of one squaring's transform at n = 5 L n2 (L = 16, n2 = 8) built from
 the same definitions as the kernels and tables (lnt_radix16.cu row5_r16,
 lnt_tables.cu launch_five_twiddles / twiddle_kernel): column transforms in
-bit-reversed row order, the 4-step twiddle omega_n^(c' brev(row)), five stride-5
-planes per row with bit-reversed L-point transforms, the twiddle
-omega_5L^(j5 brev(e)), the pair-form 5-point transform with constants
-(w^k +- w^-k)/2, the square, the inverse with outputs 1/4 and 2/3 exchanged,
-and the inverse twiddles.  Forward, square and unscaled inverse must give n
-times the cyclic self-convolution.
+bit-reversed row order, the 4-step twiddle omega_n^(c' brev(row)); in each row
+(c' = c + L j5) the pair-form 5-point transform over j5 with constants
+(w^k +- w^-k)/2, the twiddle omega_5L^(c k5), five L-point plane transforms
+(bit-reversed output), the square, and the inverse steps in reverse order (the
+inverse 5-point transform is the forward one with outputs 1/4 and 2/3
+exchanged).  Forward, square and unscaled inverse must give n times the cyclic
+self-convolution.
 """
 import random
 
@@ -73,24 +74,23 @@ def test_five_plane_squaring_is_the_cyclic_convolution():
         for row in range(n2):
             rows[row][col] = f[brev(row, lg2)] * pow(wn, col * brev(row, lg2), P) % P
     for row in range(n2):
-        planes = []
-        for j5 in range(5):
-            f = dft([rows[row][5 * cc + j5] for cc in range(L)], w_L)
-            planes.append([f[brev(e, lgL)] for e in range(L)])
-        for e in range(L):
-            k = brev(e, lgL)
-            u = [planes[j5][e] * pow(w_5L, j5 * k, P) % P for j5 in range(5)]
-            y = dft5([v * v % P for v in dft5(u, c)], c)
-            z = [y[0], y[4], y[3], y[2], y[1]]
-            for j5 in range(5):
-                planes[j5][e] = z[j5] * pow(inv(w_5L), j5 * k, P) % P
-        for j5 in range(5):
+        planes = [[0] * L for _ in range(5)]
+        for cc in range(L):
+            u = dft5([rows[row][cc + L * j5] for j5 in range(5)], c)
+            for k5 in range(5):
+                planes[k5][cc] = u[k5] * pow(w_5L, cc * k5, P) % P
+        for k5 in range(5):
+            f = dft(planes[k5], w_L)
+            sq = [f[brev(e, lgL)] ** 2 % P for e in range(L)]  # bit-reversed, squared
             nat = [0] * L
             for e in range(L):
-                nat[brev(e, lgL)] = planes[j5][e]
-            t = dft(nat, inv(w_L))
-            for cc in range(L):
-                rows[row][5 * cc + j5] = t[cc]
+                nat[brev(e, lgL)] = sq[e]
+            planes[k5] = dft(nat, inv(w_L))
+        for cc in range(L):
+            y = [planes[k5][cc] * pow(inv(w_5L), cc * k5, P) % P for k5 in range(5)]
+            z = dft5(y, c)
+            for j5, k5 in enumerate((0, 4, 3, 2, 1)):
+                rows[row][cc + L * j5] = z[k5]
     out = [0] * n
     for col in range(n1):
         freq = [0] * n2
