@@ -156,3 +156,20 @@ def test_batched_rows_per_cta(lnt, tmp_path):
         with lnt.LucasTest(q, n, False) as T:
             T.iterate(30)
             assert got[i]["status"] == 0 and got[i]["res64"] == T.res64(), q
+
+
+def test_every_row_length(lnt):
+    """n = 5 * 2^18: every plan, rows of 5 L words for L = 256 ... 4096 (the
+    largest, 174 KB of planes and 1024 threads a CTA), gives one Res64, which is
+    the Res64 of the same test at 2^21."""
+    q, n = 20000003, 5 << 18
+    plans = lnt.plan_candidates(q, n)
+    assert {p[1] for p in plans} >= {6, 10}  # n2 = 64 (L = 4096) ... 1024 (L = 256)
+    got = set()
+    for p in plans:
+        with lnt.LucasTest(q, n, False, plan=p) as T:
+            T.iterate(30)
+            got.add(T.res64())
+    with lnt.LucasTest(q, 1 << 21, False) as T:
+        T.iterate(30)
+        assert got == {T.res64()}
