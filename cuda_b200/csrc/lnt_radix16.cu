@@ -242,9 +242,9 @@ __global__ void __launch_bounds__(TH) row_mul_r16(const TwoPassDesc* __restrict_
 // pass runs with the square as in row_square_r16.  The inverse runs the same
 // steps backwards and stores the row; its factor 1/5 is in the unweights (1/n).
 
-// 5-point transform with the pair form: for u1 w^k + u4 w^-k = a1 C + b1 S
-// (a = u1 + u4, b = u1 - u4, C = (w^k + w^-k)/2, S = (w^k - w^-k)/2), eight
-// multiplications instead of sixteen.  c = {C1, C2, S1, S2}.  The inverse
+// 5-point transform with the pair form u1 w^k + u4 w^-k = a C + b S (a = u1 + u4,
+// b = u1 - u4, C = (w^k + w^-k)/2, S = (w^k - w^-k)/2; likewise u2, u3 with w^2k):
+// eight multiplications instead of sixteen.  c = {C1, C2, S1, S2}.  The inverse
 // transform (w^-1) is the same with outputs 1, 4 and 2, 3 exchanged.
 __device__ __forceinline__ void dft5(uint64_t (&u)[5], const uint64_t* c) {
   const uint64_t a1 = gl::add(u[1], u[4]), b1 = gl::sub(u[1], u[4]);
