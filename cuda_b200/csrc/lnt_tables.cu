@@ -5,8 +5,10 @@
 // reference's: w_j = 7^(((p-1)/192/n) * 5 * (n - r_j)), r_j = q j mod n, w_0 = 1,
 // uw_j = (w_j n)^-1, uw_0 = n^-1.  With g = 7^(((p-1)/192/n) * 5) (g^n = 2),
 // uw_j = g^r_j / (2n) for j > 0.  The weight of word j thus places it at bit
-// ceil(qj/n) (odd q); the widths (lnt_policy.cpp, word_widths) are the exact
-// integer differences of those bits, so every word starts where its weight says.
+// ceil(qj/n) when r_j != 0; words with r_j = 0, j > 0 (q sharing a factor with
+// n) sit exactly on bit qj/n and take weight 1.  The widths (lnt_policy.cpp,
+// word_widths) are the exact integer differences of those bits, so every word
+// starts where its weight says.
 #include "lnt_internal.h"
 #include "goldilocks.cuh"
 
@@ -24,6 +26,14 @@ __global__ void weights_kernel(uint32_t exponent, uint32_t n, uint64_t g, uint64
     return;
   }
   const uint32_t r = (uint32_t)(((uint64_t)exponent * j) % n);
+  if (r == 0) {
+    // qj/n is a whole bit: the word starts exactly there (weight 1).  The formula
+    // below would give g^n = 2, one bit off; this happens for j > 0 only when q
+    // shares a factor with n (an even q, or q divisible by 5 at n = 5 * 2^k).
+    w[j] = 1;
+    uw[j] = inv_n;
+    return;
+  }
   w[j] = gl::pow(g, (uint64_t)(n - r));
   uw[j] = gl::mul(gl::pow(g, (uint64_t)r), inv_2n);
 }

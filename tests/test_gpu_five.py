@@ -173,3 +173,18 @@ def test_every_row_length(lnt):
     with lnt.LucasTest(q, 1 << 21, False) as T:
         T.iterate(30)
         assert got == {T.res64()}
+
+
+@pytest.mark.parametrize("q,n", [(1000005, 5 << 15), (1000006, 1 << 16)])
+def test_exponents_sharing_a_factor_with_the_length(lnt, q, n):
+    """q divisible by 5 at n = 5 * 2^k (and an even q at 2^k) puts some words
+    j > 0 exactly on a whole bit (qj = 0 mod n); their weight is 1.  Digits equal
+    the big-integer model after 1, 2 and 5 squarings (PRP: any exponent)."""
+    v = random_value(q, q)
+    with lnt.LucasTest(q, n, True) as T:
+        T.set_digits(to_digits(v, q, n))
+        for k in (1, 2, 5):
+            T.iterate(k)
+            for _ in range(k):
+                v = B.step(v, q, True)
+            assert np.array_equal(T.digits(), to_digits(v, q, n)), (q, n, k)
