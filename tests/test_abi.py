@@ -96,3 +96,21 @@ def test_new_entry_points_reject_null_handles(lnt):
     assert L.lnt_jacobi_check(None, None) == 1
     assert L.lnt_jacobi_stats(None, None, None, None) == 1
     assert L.lnt_jacobi_of_digits(None, None, 0, 0, None) == 1
+    assert L.lnt_batch_short_lengths(None, 1) == 1
+
+
+def test_length_queries_reject_bad_arguments(lnt):
+    """lnt_smallest_length and lnt_shifted_words are host-only: bad pointers,
+    exponents and lengths are LNT_ERR_INVALID_ARGUMENT, an exponent past the
+    largest length LNT_ERR_UNSUPPORTED_LENGTH."""
+    import ctypes
+
+    L = lnt.lib()
+    n, c = ctypes.c_uint32(), ctypes.c_uint32()
+    assert L.lnt_smallest_length(100003, None) == 1
+    assert L.lnt_smallest_length(2, ctypes.byref(n)) == 1
+    assert L.lnt_smallest_length(2**31 - 1, ctypes.byref(n)) == 2
+    assert L.lnt_shifted_words(100003, 1 << 12, None, None) == 1
+    assert L.lnt_shifted_words(100003, 3 << 12, ctypes.byref(c), None) == 1  # not a power of two
+    assert L.lnt_shifted_words(100003, 1 << 27, ctypes.byref(c), None) == 1
+    assert L.lnt_shifted_words(100003, 1 << 12, ctypes.byref(c), None) == 0 and c.value == 0
