@@ -147,7 +147,9 @@ static bool make_five_plan(uint32_t n, uint32_t exponent, PlanOptions o, Plan& p
     if (!tile_fits(true, l2, tile)) tile = 4;
   } else if (!tile_fits(true, l2, tile)) {
     return reject("column tile must be 4 or 8 and fit shared memory");
-  } else if (exponent && tile < run_words && tile < 8) {
+  } else if (exponent && tile < run_words && tile < 8 && tile_fits(true, l2, 8)) {
+    // as the policy: 4-word runs where 8-word tiles do not fit (the kernels' carry check
+    // reports a carry that outruns them)
     return reject("carry runs of this tile are too short for the exponent");
   }
   plan.log2n1 = l1;  // log2 L: the transform length of each plane
@@ -223,7 +225,9 @@ bool make_plan(uint32_t n, uint32_t exponent, const PlanOptions* opt, Plan& plan
     if (!tile_fits(plan.fast, l2, tile)) tile = 4;
   } else if (!tile_fits(plan.fast, l2, tile)) {
     return reject("column tile must be 4 or 8 and fit shared memory");
-  } else if (exponent && tile < run_words && tile < 8) {
+  } else if (exponent && tile < run_words && tile < 8 && tile_fits(plan.fast, l2, 8)) {
+    // as the policy: 4-word runs where 8-word tiles do not fit (the kernels' carry check
+    // reports a carry that outruns them)
     return reject("carry runs of this tile are too short for the exponent");
   }
   if ((1u << l1) < tile) return reject("rows shorter than the tile");

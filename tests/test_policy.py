@@ -116,3 +116,23 @@ def test_smallest_length(lnt):
             assert n == ref
     assert 0.1 < five / len(qs) < 0.5
     assert lnt.smallest_length(170000009) == 5 << 21 and lnt.smallest_length(139000003) == 1 << 23
+
+
+def test_five_length_plans_at_every_k(lnt):
+    """Every 5 * 2^k length, 13 <= k <= 24, has register-pass plans only (radix
+    8), rows of 5 L words with 2^7 <= L <= 2^12 and columns 2^6 ... 2^12; the
+    policy takes L = 2^11 where the columns allow (2^(k-6) below k = 17, 2^12 at
+    k = 24)."""
+    for k in range(13, 25):
+        n = 5 << k
+        q = 15 * n + 1  # 15-16 bits a word: within the bound at every k here
+        plans = lnt.plan_candidates(q, n)
+        assert plans and all(p[0] == 2 and p[3] == 8 for p in plans), k
+        for p in plans:
+            name = lnt.plan_describe(p, q, n)
+            n2, rest = name.split("_")[1].split("x", 1)
+            L = int(rest.split("x")[1])
+            assert rest.startswith("5x") and int(n2) * 5 * L == n
+            assert 64 <= int(n2) <= 4096 and 128 <= L <= 4096
+        policy_L = int(lnt.plan_describe(plans[0], q, n).split("_")[1].split("x")[2])
+        assert policy_L == (1 << min(11, k - 6) if k < 24 else 1 << 12), k
