@@ -6,6 +6,8 @@
  *
  * Every function restates one piece of the reference (LucasNTT/cuda); the
  * citation in front of each function is the reference file:line it follows.
+ * One section has no reference counterpart and says so: lengths n = 5 * 2^k,
+ * the checker of the library's own extension, pinned to the big-integer model.
  * The arithmetic is exact uint64 arithmetic modulo the Goldilocks prime
  * p = 2^64 - 2^32 + 1, written here from the algebra (2^64 = 2^32 - 1 and
  * 2^96 = -1 mod p), not transcribed.
@@ -244,9 +246,123 @@ typedef struct {
     int prp;
     uint64_t *w, *uw, *rt, *irt, *x;
     uint8_t* widths;
+    /* n = 5 m (m = 2^k): no reference counterpart (its Length names factors of
+     * 5 but no kernel runs them).  rt/irt are then the roots of the m-point
+     * plane transforms, tw5[(k5 - 1) m + c] = omega_n^(c k5), c5 the pair-form
+     * constants of the 5-point transform (omega_5 = omega_n^m). */
+    uint32_t m;
+    uint64_t *tw5, *itw5, c5[4];
 } oracle_ctx;
 
+/* ---- lengths n = 5 * 2^k (not a reference path) --------------------------
+ *
+ * Same arithmetic as the power-of-two path except the transform and two table
+ * details, both written for this length only: the widths are exact integers
+ * (ceil(q(j+1)/n) - ceil(qj/n); the double expression can be off once q*j
+ * passes 2^53), and a word with qj = 0 mod n, j > 0, sits on a whole bit and
+ * takes weight 1 (the power-of-two formula would give g^n = 2).  The transform
+ * of x (c' = c + m j5) is X[5 km + k5] =
+ *   sum_c omega_m^(c km) omega_n^(c k5) sum_j5 omega_5^(j5 k5) x[c + m j5]:
+ * a 5-point transform per c, a twiddle, and five m-point transforms. */
+
+static void dft5(uint64_t u[5], const uint64_t c[4]) {
+    uint64_t a1 = gl_add(u[1], u[4]), b1 = gl_sub(u[1], u[4]);
+    uint64_t a2 = gl_add(u[2], u[3]), b2 = gl_sub(u[2], u[3]);
+    uint64_t t1 = gl_add(gl_mul(a1, c[0]), gl_mul(a2, c[1]));
+    uint64_t t2 = gl_add(gl_mul(a1, c[1]), gl_mul(a2, c[0]));
+    uint64_t s1 = gl_add(gl_mul(b1, c[2]), gl_mul(b2, c[3]));
+    uint64_t s2 = gl_sub(gl_mul(b1, c[3]), gl_mul(b2, c[2]));
+    uint64_t u0 = u[0];
+    u[0] = gl_add(u0, gl_add(a1, a2));
+    u[1] = gl_add(gl_add(u0, t1), s1);
+    u[4] = gl_sub(gl_add(u0, t1), s1);
+    u[2] = gl_add(gl_add(u0, t2), s2);
+    u[3] = gl_sub(gl_add(u0, t2), s2);
+}
+
+static void* oracle_create_five(uint32_t exponent, uint32_t n, int prp) {
+    uint32_t m = n / 5;
+    oracle_ctx* c = (oracle_ctx*)calloc(1, sizeof(oracle_ctx));
+    c->q = exponent; c->n = n; c->prp = prp; c->m = m;
+    c->w = (uint64_t*)malloc(8ULL * n);
+    c->uw = (uint64_t*)malloc(8ULL * n);
+    c->x = (uint64_t*)calloc(n, 8);
+    c->rt = (uint64_t*)malloc(8ULL * (m / 2 ? m / 2 : 1));
+    c->irt = (uint64_t*)malloc(8ULL * (m / 2 ? m / 2 : 1));
+    c->widths = (uint8_t*)malloc(n);
+    c->tw5 = (uint64_t*)malloc(8ULL * 4 * m);
+    c->itw5 = (uint64_t*)malloc(8ULL * 4 * m);
+    uint64_t g = oracle_gl_pow(7, ((GL_P - 1) / 192 / n) * 5ULL);
+    uint64_t inv_n = oracle_gl_inv(n), inv_2n = oracle_gl_inv(2ULL * n);
+    uint64_t prev = 0;
+    for (uint32_t j = 0; j < n; j++) {
+        uint64_t next = ((uint64_t)exponent * (j + 1) + n - 1) / n;
+        c->widths[j] = (uint8_t)(next - prev);
+        prev = next;
+        uint64_t r = ((uint64_t)exponent * j) % n;
+        if (r == 0) {
+            c->w[j] = 1;
+            c->uw[j] = inv_n;
+        } else {
+            c->w[j] = oracle_gl_pow(g, n - r);
+            c->uw[j] = gl_mul(oracle_gl_pow(g, r), inv_2n);
+        }
+    }
+    make_roots(m, c->rt, c->irt);
+    uint64_t wn = oracle_gl_pow(554, (GL_P - 1) / n), iwn = oracle_gl_inv(wn);
+    for (uint32_t k5 = 1; k5 < 5; k5++)
+        for (uint32_t cc = 0; cc < m; cc++) {
+            c->tw5[(k5 - 1) * m + cc] = oracle_gl_pow(wn, (uint64_t)cc * k5);
+            c->itw5[(k5 - 1) * m + cc] = oracle_gl_pow(iwn, (uint64_t)cc * k5);
+        }
+    uint64_t w5 = oracle_gl_pow(wn, m), half = oracle_gl_inv(2);
+    uint64_t w2 = gl_mul(w5, w5), w3 = gl_mul(w2, w5), w4 = gl_mul(w3, w5);
+    c->c5[0] = gl_mul(gl_add(w5, w4), half);
+    c->c5[1] = gl_mul(gl_add(w2, w3), half);
+    c->c5[2] = gl_mul(gl_sub(w5, w4), half);
+    c->c5[3] = gl_mul(gl_sub(w2, w3), half);
+    c->x[0] = prp ? 3 : 4;
+    return c;
+}
+
+/* forward transform, pointwise square, unscaled inverse (factor n in uw) */
+static void five_square(oracle_ctx* c) {
+    uint32_t m = c->m;
+    uint64_t* x = c->x;
+    uint64_t* y = (uint64_t*)malloc(8ULL * c->n);
+    #pragma omp parallel for schedule(static) if (m >= (1u << 12))
+    for (int64_t cc = 0; cc < (int64_t)m; cc++) {
+        uint64_t u[5];
+        for (int j5 = 0; j5 < 5; j5++) u[j5] = x[cc + (uint64_t)m * j5];
+        dft5(u, c->c5);
+        y[cc] = u[0];
+        for (int k5 = 1; k5 < 5; k5++) y[(uint64_t)k5 * m + cc] = gl_mul(u[k5], c->tw5[(k5 - 1) * m + cc]);
+    }
+    for (int k5 = 0; k5 < 5; k5++) {
+        uint64_t* plane = y + (uint64_t)k5 * m;
+        ntt_dif(plane, m, c->rt);
+        for (uint32_t e = 0; e < m; e++) plane[e] = gl_mul(plane[e], plane[e]);
+        intt_dit(plane, m, c->irt);
+    }
+    #pragma omp parallel for schedule(static) if (m >= (1u << 12))
+    for (int64_t cc = 0; cc < (int64_t)m; cc++) {
+        uint64_t u[5];
+        u[0] = y[cc];
+        for (int k5 = 1; k5 < 5; k5++) u[k5] = gl_mul(y[(uint64_t)k5 * m + cc], c->itw5[(k5 - 1) * m + cc]);
+        dft5(u, c->c5);
+        x[cc] = u[0];
+        x[cc + m] = u[4];
+        x[cc + 2ULL * m] = u[3];
+        x[cc + 3ULL * m] = u[2];
+        x[cc + 4ULL * m] = u[1];
+    }
+    free(y);
+}
+
+static int is_pow2(uint32_t n) { return n >= 2 && (n & (n - 1)) == 0; }
+
 void* oracle_create(uint32_t exponent, uint32_t n, int prp) {
+    if (n % 5 == 0 && is_pow2(n / 5) && n <= (5u << 24)) return oracle_create_five(exponent, n, prp);
     if (n < 2 || (n & (n - 1)) || n > (1u << 26)) return NULL;
     oracle_ctx* c = (oracle_ctx*)calloc(1, sizeof(oracle_ctx));
     c->q = exponent; c->n = n; c->prp = prp;
@@ -267,6 +383,7 @@ void oracle_destroy(void* p) {
     oracle_ctx* c = (oracle_ctx*)p;
     if (!c) return;
     free(c->w); free(c->uw); free(c->x); free(c->rt); free(c->irt); free(c->widths);
+    free(c->tw5); free(c->itw5);
     free(c);
 }
 
@@ -326,10 +443,14 @@ int oracle_iterate(void* p, uint64_t iterations) {
     for (uint64_t it = 0; it < iterations; it++) {
         #pragma omp parallel for schedule(static) if (n >= (1u << 15))
         for (int64_t j = 0; j < (int64_t)n; j++) x[j] = gl_mul(x[j], c->w[j]);
-        ntt_dif(x, n, c->rt);
-        #pragma omp parallel for schedule(static) if (n >= (1u << 15))
-        for (int64_t j = 0; j < (int64_t)n; j++) x[j] = gl_mul(x[j], x[j]);
-        intt_dit(x, n, c->irt);
+        if (c->m) {
+            five_square(c);
+        } else {
+            ntt_dif(x, n, c->rt);
+            #pragma omp parallel for schedule(static) if (n >= (1u << 15))
+            for (int64_t j = 0; j < (int64_t)n; j++) x[j] = gl_mul(x[j], x[j]);
+            intt_dit(x, n, c->irt);
+        }
         #pragma omp parallel for schedule(static) if (n >= (1u << 15))
         for (int64_t j = 0; j < (int64_t)n; j++) x[j] = gl_mul(x[j], c->uw[j]);
         if (reduce_to_base(x, c->widths, n) != 0) return -1;

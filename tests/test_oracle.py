@@ -149,3 +149,30 @@ def test_oracle_matches_reference_build_prp_and_batch_pins(oracle_mod):
             T.iterate(c["iterations"])
             assert f"{T.res64():016x}" == c["res64"], c
 
+
+
+@pytest.mark.parametrize("q,n,prp", [(3001, 320, False), (3001, 320, True), (20011, 2560, False),
+                                     (100005, 10240, True), (100003, 10240, False)])
+def test_five_length_oracle_matches_bigint_model(oracle_mod, q, n, prp):
+    """The oracle's n = 5 * 2^k path (no reference counterpart: exact widths, a
+    5-point step and five power-of-two transforms) gives the big-integer model's
+    digits from a random state, q = 100005 (divisible by 5: words on whole bits)
+    included."""
+    import random
+
+    rng = random.Random(q + n)
+    v = rng.randrange((1 << q) - 1)
+    with oracle_mod.OracleTest(q, n, prp) as O:
+        assert O.widths().tolist() == B.widths(q, n)
+        O.set_digits(np.array(B.to_digits(v, q, n), dtype=np.uint64))
+        for k in (1, 2, 3):
+            O.iterate(k)
+            for _ in range(k):
+                v = B.step(v, q, prp)
+            assert O.digits().tolist() == B.to_digits(v, q, n), k
+
+
+def test_five_length_oracle_known_prime(oracle_mod):
+    with oracle_mod.OracleTest(9941, 640, False) as O:
+        O.iterate(9939)
+        assert O.is_prime() and O.res64() == 0
