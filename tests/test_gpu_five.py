@@ -188,3 +188,19 @@ def test_exponents_sharing_a_factor_with_the_length(lnt, q, n):
             for _ in range(k):
                 v = B.step(v, q, True)
             assert np.array_equal(T.digits(), to_digits(v, q, n)), (q, n, k)
+
+
+@pytest.mark.parametrize("q,n,prp", [(300007, 5 << 13, False), (1000005, 5 << 15, True),
+                                     (2000003, 5 << 16, False)])
+def test_digits_equal_oracle(lnt, oracle_mod, q, n, prp):
+    """Digit for digit against the oracle's 5 * 2^k path after 1 and 3 squarings
+    from a random canonical state."""
+    start = to_digits(random_value(q, n), q, n)
+    with lnt.LucasTest(q, n, prp) as T, oracle_mod.OracleTest(q, n, prp) as O:
+        T.set_digits(start)
+        O.set_digits(start)
+        for k in (1, 3):
+            T.iterate(k)
+            O.iterate(k)
+            assert np.array_equal(T.digits(), O.digits()), (q, n, prp, k)
+        assert T.res64() == O.res64()
